@@ -1,0 +1,339 @@
+"""Benchmark of the fused FP64 mass operator_apply (GDoF/s) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Workload (one GPU): the order-sweep mesh of ~64M DoFs -- a perturbed 3D hex
+box of 100^3 elements on [0,1]^3, P=5 GLL nodes and Q=6 Gauss points per
+direction, num_comp=1, FP64, u ~ U[-1,1] (seeded), qdata = det(J) w built on
+the device.  A step is one operator apply v = M u over the whole mesh (v
+zeroed, then the fused gather/interp/qfunction/interp^T/scatter-add kernel).
+Inputs (3.3 GB per apply) exceed the 126 MB L2, so no flush is needed between
+steps.  With N ranks (torchrun) each GPU applies its own copy of the mesh
+(independent meshes, no collective on the data path): weak scaling, value =
+all ranks' DoFs / max-over-ranks time.
+
+--impl reference times the reference CPU implementation (fe-demo-cpp's own
+operator_apply, compiled from its sources into oracle/_ref) with all host
+threads, on a bounded sample of the same workload; rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "GDoF/s operator_apply"
+UNIT = "GDoF/s"
+SHAPE, P, Q, NC, SEED = (100, 100, 100), 5, 6, 1, 1
+WORKLOAD = ("mass operator_apply, FP64 3D hex box 100^3 elements on [0,1]^3 (interior vertices "
+            "perturbed U[-0.1h,0.1h], seed 1), P=5 GLL nodes, Q=6 Gauss points, num_comp=1, "
+            "~64.5M DoFs, qdata = det(J)*w, u ~ U[-1,1]")
+
+
+def algorithmic_bytes(num_elem, num_nodes, P, Q, nc=1, dim=3):
+    """Compulsory HBM bytes of one fused apply: offsets (int32) and qdata (FP64)
+    per element, u read + v write per DoF."""
+    return num_elem * (4 * P**dim + 8 * Q**dim) + 16 * nc * num_nodes
+
+
+def algorithmic_flops(num_elem, P, Q, nc=1):
+    """Sum-factorised flops of one apply (3D): interp + interp^T + pointwise."""
+    return num_elem * nc * (4 * (P**3 * Q + P**2 * Q**2 + P * Q**3) + Q**3)
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return d["hbm_gbs"], "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """DRAM bytes per launch of the fused kernel from the committed ncu summary
+    (profiles/mass3d_apply_P5Q6_64M.md, line 'dram_bytes_per_launch: <n>')."""
+    path = os.path.join(ROOT, "profiles", "mass3d_apply_P5Q6_64M.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.strip().startswith("dram_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+# ---------------------------------------------------------------------------
+# reference CPU path on a bounded sample
+# ---------------------------------------------------------------------------
+class RefSample:
+    """The first `n_slabs` z-layers of elements of the workload mesh as a
+    self-contained mesh, applied by the reference's operator_apply on element
+    chunks in parallel threads (oracle.RefPlan)."""
+
+    def __init__(self, mesh, target_s=2.0, threads=None):
+        import oracle
+        self.oracle = oracle
+        oracle.build(with_ref=None)
+        self.ref = oracle.ref()
+        self.mesh = mesh
+        self.threads = threads or host_threads()
+        slab = mesh.shape[0] * mesh.shape[1]
+        # calibrate on one slab, then size the sample to ~target_s per apply
+        self._make(1)
+        self._time_once()
+        t = self._time_once()
+        self.close()
+        slabs = int(max(1, min(mesh.shape[2], round(target_s / max(t, 1e-3)))))
+        self.n_slabs = slabs
+        self.ne = self._make(slabs)
+        self.frac = self.ne / mesh.num_elem
+
+    def _make(self, slabs):
+        m = self.mesh
+        ne = slabs * m.shape[0] * m.shape[1]
+        local, n_loc, _, coords = self.oracle.compact_submesh(m.offsets, P**3, ne, m.coords, 3, m.num_nodes)
+        # qdata through the reference build operator, per chunk in parallel
+        self.plan = self.oracle.RefPlan(self.ref, 3, ne, P, Q, n_loc, local, None, self.threads, coords=coords)
+        self.u = np.random.default_rng([SEED, 1]).uniform(-1, 1, n_loc)
+        self.v = np.zeros(n_loc)
+        return ne
+
+    def _time_once(self):
+        t0 = time.perf_counter()
+        self.plan.apply(self.u, self.v)
+        return time.perf_counter() - t0
+
+    def gdofs(self, seconds):
+        # scaled to the whole workload by the element fraction of the sample
+        return self.mesh.num_nodes * self.frac / seconds / 1e9
+
+    def describe(self):
+        return (f"first {self.n_slabs} of {self.mesh.shape[2]} z-slabs ({self.ne} of {self.mesh.num_elem} elements, "
+                f"{self.frac:.1%}) through the reference operator_apply, {self.threads} threads, element-chunked; "
+                f"GDoF/s scaled by the element fraction")
+
+    def close(self):
+        if getattr(self, "plan", None) is not None:
+            self.plan.close()
+            self.plan = None
+
+
+def run_reference(args, rank):
+    from fe_demo_cpp_b200.mesh import box_mesh
+    if rank != 0:
+        return None
+    mesh = box_mesh(SHAPE, P, seed=SEED)
+    # each step is a sample sized so that warm-up + steps take about two minutes
+    s = RefSample(mesh, target_s=min(2.0, 120.0 / (args.steps + args.warmup)))
+    for _ in range(args.warmup):
+        s._time_once()
+    times = [s._time_once() for _ in range(args.steps)]
+    s.close()
+    t = statistics.median(times)
+    value = s.gdofs(t)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "mesh": "x".join(map(str, SHAPE)), "P": P, "Q": Q, "num_comp": NC,
+                   "dofs": mesh.num_nodes, "parallelism": "host threads over element chunks"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": s.threads, "kind": "reference",
+                         "sample": s.describe()},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    return line
+
+
+# ---------------------------------------------------------------------------
+# the device path
+# ---------------------------------------------------------------------------
+def run_b200(args, rank, world, local_rank):
+    import torch
+    import fe_demo_cpp_b200 as fem
+    from fe_demo_cpp_b200.build import build
+    from fe_demo_cpp_b200.mesh import box_mesh
+    from fe_demo_cpp_b200.telemetry import ClockSampler
+
+    build()
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    stream = torch.cuda.current_stream()
+
+    mesh = box_mesh(SHAPE, P, seed=SEED)
+    N, ne = mesh.num_nodes, mesh.num_elem
+    x = torch.from_numpy(mesh.coords).to(dev)
+    rx = fem.Restriction(ne, P**3, 3, N, 3 * N, mesh.offsets)
+    bx = fem.Basis(3, 3, P, Q)
+    qdata = torch.empty(Q**3 * ne, dtype=torch.float64, device=dev)
+    fem.mass_build(rx, bx, x, qdata)
+    ru = fem.Restriction(ne, P**3, 1, N, N, mesh.offsets)
+    bu = fem.Basis(3, 1, P, Q)
+    op = fem.MassOperator(ru, bu, qdata)
+    launches = op.info()["launches_per_apply"]
+    del x, rx, bx, qdata
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+
+    g = torch.Generator(device=dev).manual_seed(SEED + rank)
+    u = torch.rand(N, dtype=torch.float64, device=dev, generator=g) * 2 - 1
+    v = torch.empty(N, dtype=torch.float64, device=dev)
+    w = torch.zeros(N, dtype=torch.float64, device=dev)
+
+    for _ in range(max(3, args.warmup)):
+        op.apply(u, v)
+        op.apply_add(u, w)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+
+    K = args.steps
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(K + 1)] for _ in range(2)]
+    sampler = ClockSampler(local_rank).start()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    # timed region 1: the public apply (zero v + fused kernel), per step
+    for i in range(K):
+        ev[0][i].record(stream)
+        op.apply(u, v)
+    ev[0][K].record(stream)
+    # timed region 2: the fused kernel alone (apply_add: no zeroing)
+    for i in range(K):
+        ev[1][i].record(stream)
+        op.apply_add(u, w)
+    ev[1][K].record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = sampler.stop()
+    step_ms = [ev[0][i].elapsed_time(ev[0][i + 1]) for i in range(K)]
+    kern_ms = [ev[1][i].elapsed_time(ev[1][i + 1]) for i in range(K)]
+    t_step = sum(step_ms) / K
+    t_kern = sum(kern_ms) / K
+    if dist:
+        t = torch.tensor([t_step, t_kern], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_step, t_kern = t.tolist()
+    value = world * N / (t_step * 1e-3) / 1e9
+
+    # end to end through the host-memory entry point: pinned u in, v out
+    u_h = torch.empty(N, dtype=torch.float64, pin_memory=True)
+    v_h = torch.empty(N, dtype=torch.float64, pin_memory=True)
+    u_h.copy_(u.cpu())
+    for _ in range(2):
+        op.apply_host(u_h.numpy(), v_h.numpy())
+    e2e_steps = max(3, min(K, 20))
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        op.apply_host(u_h.numpy(), v_h.numpy())
+    t_e2e = (time.perf_counter() - t0) / e2e_steps
+    if dist:
+        t = torch.tensor([t_e2e], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_e2e = t.item()
+    e2e_value = world * N / t_e2e / 1e9
+    # e2e parity guard: the host path returns the device result
+    assert np.array_equal(v_h.numpy(), v.cpu().numpy()) or np.abs(v_h.numpy() - v.cpu().numpy()).max() <= 1e-13 * np.abs(v.cpu().numpy()).max()
+
+    peak, peak_kind = measured_peaks()
+    abytes = algorithmic_bytes(ne, N, P, Q)
+    achieved = abytes / (t_kern * 1e-3) / 1e9
+    traffic = ncu_traffic()
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup,
+        "ms_per_step": t_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "mesh": "x".join(map(str, SHAPE)), "P": P, "Q": Q, "num_comp": NC,
+                   "dofs": N, "elements": ne, "scatter": "atomic", "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (3.3 GB per apply); no flush",
+                   "kernel": "mass3d_apply_kernel<5,6>", "kernel_ms": t_kern,
+                   "algorithmic_bytes_per_apply": abytes,
+                   "algorithmic_flops_per_apply": algorithmic_flops(ne, P, Q)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
+                     if peak_kind == "measured" else "fallback 6650 GB/s"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * N, "d2h_bytes_per_step": 8 * N,
+                "path": "fem_b200_mass_apply_host (pinned host u in, v out, synchronous)"},
+        "clocks": clocks,
+        "gpu_launches": 2 * K * launches,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        s = RefSample(mesh, target_s=args.cpu_sample_s / 4)
+        s._time_once()
+        ts = [s._time_once() for _ in range(3)]
+        s.close()
+        line["cpu_baseline"] = {"value": s.gdofs(statistics.median(ts)), "unit": UNIT, "cores": s.threads,
+                                "kind": "reference", "sample": s.describe() + ", median of 3 after 1 warm-up"}
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample-s", type=float, default=12.0, help="approximate CPU seconds of the baseline")
+    ap.add_argument("--shape", default=None, help="elements per direction nx,ny,nz (default 100,100,100)")
+    ap.add_argument("--P", type=int, default=None, help="nodes per direction (Q = P+1)")
+    args = ap.parse_args()
+    global SHAPE, P, Q, WORKLOAD
+    if args.shape or args.P:
+        SHAPE = tuple(int(s) for s in args.shape.split(",")) if args.shape else SHAPE
+        P = args.P or P
+        Q = P + 1
+        WORKLOAD = (f"mass operator_apply, FP64 3D hex box {'x'.join(map(str, SHAPE))} elements (perturbed, "
+                    f"seed 1), P={P}, Q={Q}, num_comp=1 (non-default size)")
+    args.warmup = max(3, args.warmup)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        line = run_reference(args, rank)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        return 0
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local_rank))
+    line = run_b200(args, rank, world, local_rank)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

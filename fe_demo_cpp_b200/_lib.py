@@ -1,0 +1,89 @@
+"""ctypes binding of libfem_b200.so (the C ABI in include/fem_b200.h).
+
+The library is built in-tree by ``python -m fe_demo_cpp_b200.build``.  There
+is no fallback: if the library is missing, loading fails with an error that
+says how to build it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "lib", "libfem_b200.so")
+
+SUCCESS, ERROR_ARGUMENT, ERROR_CUDA, ERROR_UNSUPPORTED = 0, 1, 2, 3
+
+_i, _i64, _p, _dp, _ip = C.c_int, C.c_int64, C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int)
+
+# name -> argtypes (every entry point of include/fem_b200.h)
+SIGNATURES = {
+    "fem_b200_last_error": ([], C.c_char_p),
+    "fem_b200_version": ([], _i),
+    "fem_b200_device_count": ([], _i),
+    "fem_b200_gauss_legendre": ([_i, _p, _p], _i),
+    "fem_b200_gauss_lobatto": ([_i, _p, _p], _i),
+    "fem_b200_lagrange_basis_matrix": ([_i, _p, _i, _p, _p, _p], _i),
+    "fem_b200_tensor_h1_lagrange": ([_i, _i, _i, _i, _i, _p, _p, _p, _p], _i),
+    "fem_b200_restriction_check_offset": ([_i, _i, _i, _i, _i, _p, _i64], _i),
+    "fem_b200_restriction_check_strided": ([_i, _i, _i, _i, _p], _i),
+    "fem_b200_transpose_map": ([_i, _i, _i, _p, _p, _p, _p, _p], _i),
+    "fem_b200_restriction_create_offset": ([_i, _i, _i, _i, _i, _p, _i, _p], _i),
+    "fem_b200_restriction_create_strided": ([_i, _i, _i, _i, _p, _p], _i),
+    "fem_b200_restriction_destroy": ([_p], _i),
+    "fem_b200_restriction_sizes": ([_p, _p, _p, _p, _p, _p], _i),
+    "fem_b200_restriction_transpose_map": ([_p, _p, _p, _p, _p], _i),
+    "fem_b200_restriction_apply": ([_p, _i, _p, _i64, _p, _i64, _p], _i),
+    "fem_b200_restriction_multiplicity": ([_p, _p, _i64, _p], _i),
+    "fem_b200_basis_create": ([_i, _i, _i, _i, _i, _p], _i),
+    "fem_b200_basis_destroy": ([_p], _i),
+    "fem_b200_basis_apply": ([_p, _i, _i, _i, _p, _i64, _p, _i64, _p], _i),
+    "fem_b200_mass_build": ([_p, _p, _p, _i64, _p, _i64, _p], _i),
+    "fem_b200_mass_create": ([_p, _p, _p, _i64, _i, _p], _i),
+    "fem_b200_mass_destroy": ([_p], _i),
+    "fem_b200_mass_apply": ([_p, _p, _i64, _p, _i64, _p], _i),
+    "fem_b200_mass_apply_add": ([_p, _p, _i64, _p, _i64, _p], _i),
+    "fem_b200_mass_apply_host": ([_p, _p, _i64, _p, _i64, _p], _i),
+    "fem_b200_mass_info": ([_p, _p, _p, _p], _i),
+}
+
+_lib = None
+
+
+class FemError(RuntimeError):
+    """A CUDA or device-path failure reported by libfem_b200."""
+
+
+class FemUnsupported(FemError):
+    """A valid request the device path does not implement (no CPU fallback)."""
+
+
+def load(path: str = LIB_PATH) -> C.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FemError(f"{path} is missing: build it with `python -m fe_demo_cpp_b200.build` "
+                       "(there is no CPU fallback)")
+    lib = C.CDLL(path)
+    for name, (argtypes, restype) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = argtypes
+        fn.restype = restype
+    _lib = lib
+    return lib
+
+
+def check(rc: int) -> None:
+    if rc == SUCCESS:
+        return
+    msg = load().fem_b200_last_error().decode()
+    if rc == ERROR_ARGUMENT:
+        raise ValueError(msg)
+    if rc == ERROR_UNSUPPORTED:
+        raise FemUnsupported(msg)
+    raise FemError(msg)
+
+
+def call(name: str, *args) -> None:
+    check(getattr(load(), name)(*args))

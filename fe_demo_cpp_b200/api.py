@@ -1,0 +1,273 @@
+"""Python objects over the libfem_b200 C ABI (tests, benchmarks, scripting).
+
+Device arrays are torch CUDA tensors (float64 / int32, contiguous); host
+arrays are numpy.  Each object owns one C handle and releases it on close()
+or garbage collection.  Names follow the reference API (fe-demo-cpp):
+restriction gather/scatter, tensor basis, the mass operator and its
+geometric-factor build.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from enum import IntEnum
+
+import numpy as np
+
+from . import _lib
+from ._lib import call
+
+
+class ContractMode(IntEnum):
+    NoTranspose = 0
+    Transpose = 1
+
+
+class EvalMode(IntEnum):
+    None_ = 0
+    Interp = 1
+    Grad = 2
+    Weight = 3
+
+
+class QuadMode(IntEnum):
+    Gauss = 0
+    GaussLobatto = 1
+
+
+class ScatterMode(IntEnum):
+    Atomic = 0
+    Deterministic = 1
+
+
+class QF(IntEnum):
+    """Device QFunctions of the mass operator."""
+    apply_mass = 0          # the reference apply_mass: component 0 only
+    apply_mass_vector = 1   # every component
+
+
+def _ptr(a) -> int:
+    if a is None:
+        return 0
+    if isinstance(a, np.ndarray):
+        if not a.flags["C_CONTIGUOUS"]:
+            raise ValueError("array must be contiguous")
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):
+        if not a.is_contiguous():
+            raise ValueError("tensor must be contiguous")
+        return a.data_ptr()
+    return int(a)
+
+
+def _n(a) -> int:
+    return int(a.size) if isinstance(a, np.ndarray) else int(a.numel())
+
+
+def _check_dev(a, dtype_name="float64"):
+    if a is None:
+        return
+    if isinstance(a, np.ndarray) or not getattr(a, "is_cuda", False):
+        raise ValueError("expected a CUDA tensor")
+    if str(a.dtype) != f"torch.{dtype_name}":
+        raise ValueError(f"expected a {dtype_name} tensor, got {a.dtype}")
+
+
+def _stream(stream) -> int:
+    if stream is None:
+        import torch
+        return torch.cuda.current_stream().cuda_stream
+    return int(getattr(stream, "cuda_stream", stream))
+
+
+# ---------------------------------------------------------------------------
+# host set-up (no GPU)
+# ---------------------------------------------------------------------------
+def gauss_legendre_quadrature(Q: int):
+    x, w = np.zeros(max(Q, 0)), np.zeros(max(Q, 0))
+    call("fem_b200_gauss_legendre", Q, _ptr(x), _ptr(w))
+    return x, w
+
+
+def gauss_lobatto_points(Q: int, weights: bool = False):
+    x, w = np.zeros(max(Q, 1)), np.zeros(max(Q, 1))
+    call("fem_b200_gauss_lobatto", Q, _ptr(x), _ptr(w) if weights else 0)
+    return (x, w) if weights else x
+
+
+def lagrange_basis_matrix(nodes, eval_points):
+    nodes = np.ascontiguousarray(nodes, dtype=np.float64)
+    pts = np.ascontiguousarray(eval_points, dtype=np.float64)
+    B = np.zeros(len(pts) * len(nodes))
+    G = np.zeros_like(B)
+    call("fem_b200_lagrange_basis_matrix", len(nodes), _ptr(nodes), len(pts), _ptr(pts), _ptr(B), _ptr(G))
+    return B, G
+
+
+def tensor_h1_lagrange(dim, num_comp, P, Q, quad_mode=QuadMode.Gauss):
+    """(q_ref[Q], q_weight[Q], interp[Q*P], grad[Q*P]) of the tensor H1 Lagrange basis."""
+    q, w = np.zeros(max(Q, 1)), np.zeros(max(Q, 1))
+    B, G = np.zeros(max(Q * P, 1)), np.zeros(max(Q * P, 1))
+    call("fem_b200_tensor_h1_lagrange", dim, num_comp, P, Q, int(quad_mode), _ptr(q), _ptr(w), _ptr(B), _ptr(G))
+    return q[:Q], w[:Q], B[:Q * P], G[:Q * P]
+
+
+def check_offset_restriction(num_elem, elem_size, num_comp, comp_stride, l_size, offsets) -> None:
+    offsets = np.ascontiguousarray(offsets, dtype=np.int32)
+    call("fem_b200_restriction_check_offset", num_elem, elem_size, num_comp, comp_stride, l_size, _ptr(offsets),
+         offsets.size)
+
+
+def check_strided_restriction(num_elem, elem_size, num_comp, l_size, strides=None) -> None:
+    s = None if strides is None else np.ascontiguousarray(strides, dtype=np.int32)
+    call("fem_b200_restriction_check_strided", num_elem, elem_size, num_comp, l_size, _ptr(s))
+
+
+def transpose_map(num_elem, elem_size, l_size, offsets):
+    """(l_vec_indices, t_offsets, t_indices) of an offset restriction, on the host."""
+    offsets = np.ascontiguousarray(offsets, dtype=np.int32)
+    lvi = np.zeros(l_size, np.int32)
+    to = np.zeros(l_size + 1, np.int32)
+    ti = np.zeros(max(num_elem * elem_size, 1), np.int32)
+    n = C.c_int(0)
+    call("fem_b200_transpose_map", num_elem, elem_size, l_size, _ptr(offsets), _ptr(lvi), _ptr(to), _ptr(ti),
+         C.addressof(n))
+    return lvi[:n.value].copy(), to[:n.value + 1].copy(), ti[:num_elem * elem_size].copy()
+
+
+# ---------------------------------------------------------------------------
+# device objects
+# ---------------------------------------------------------------------------
+class _Handle:
+    _destroy = ""
+
+    def __init__(self):
+        self.h = C.c_void_p(0)
+
+    def close(self):
+        if self.h and self.h.value:
+            _lib.load()
+            getattr(_lib.load(), self._destroy)(self.h)
+            self.h = C.c_void_p(0)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+class Restriction(_Handle):
+    """Device element restriction (offset or strided)."""
+    _destroy = "fem_b200_restriction_destroy"
+
+    def __init__(self, num_elem, elem_size, num_comp, comp_stride, l_size, offsets,
+                 scatter_mode=ScatterMode.Atomic):
+        super().__init__()
+        offsets = np.ascontiguousarray(offsets, dtype=np.int32)
+        call("fem_b200_restriction_create_offset", num_elem, elem_size, num_comp, comp_stride, l_size,
+             _ptr(offsets), int(scatter_mode), C.addressof(self.h))
+        self.strided = False
+        self.num_elem, self.elem_size, self.num_comp = num_elem, elem_size, num_comp
+        self.comp_stride, self.l_size = comp_stride, l_size
+        self.e_size = num_comp * elem_size * num_elem
+        self.scatter_mode = ScatterMode(scatter_mode)
+
+    @classmethod
+    def strided_create(cls, num_elem, elem_size, num_comp, l_size, strides=None):
+        self = cls.__new__(cls)
+        _Handle.__init__(self)
+        s = None if strides is None else np.ascontiguousarray(strides, dtype=np.int32)
+        call("fem_b200_restriction_create_strided", num_elem, elem_size, num_comp, l_size, _ptr(s),
+             C.addressof(self.h))
+        self.strided = True
+        self.num_elem, self.elem_size, self.num_comp = num_elem, elem_size, num_comp
+        self.comp_stride, self.l_size = 0, l_size
+        self.e_size = num_comp * elem_size * num_elem
+        self.scatter_mode = ScatterMode.Atomic
+        return self
+
+    def apply(self, t_mode, inp, out, stream=None):
+        """NoTranspose: out = E in (overwritten).  Transpose: out += E^T in."""
+        _check_dev(inp)
+        _check_dev(out)
+        call("fem_b200_restriction_apply", self.h, int(t_mode), _ptr(inp), _n(inp), _ptr(out), _n(out),
+             _stream(stream))
+
+    def multiplicity(self, mult, stream=None):
+        _check_dev(mult)
+        call("fem_b200_restriction_multiplicity", self.h, _ptr(mult), _n(mult), _stream(stream))
+
+    def transpose_map(self):
+        lvi = np.zeros(self.l_size, np.int32)
+        to = np.zeros(self.l_size + 1, np.int32)
+        ti = np.zeros(self.num_elem * self.elem_size, np.int32)
+        n = C.c_int(0)
+        call("fem_b200_restriction_transpose_map", self.h, _ptr(lvi), _ptr(to), _ptr(ti), C.addressof(n))
+        return lvi[:n.value].copy(), to[:n.value + 1].copy(), ti
+
+
+class Basis(_Handle):
+    """Device tensor-product H1 Lagrange basis."""
+    _destroy = "fem_b200_basis_destroy"
+
+    def __init__(self, dim, num_comp, P, Q, quad_mode=QuadMode.Gauss):
+        super().__init__()
+        call("fem_b200_basis_create", dim, num_comp, P, Q, int(quad_mode), C.addressof(self.h))
+        self.dim, self.num_comp, self.P, self.Q, self.quad_mode = dim, num_comp, P, Q, QuadMode(quad_mode)
+
+    def host_data(self):
+        return tensor_h1_lagrange(self.dim, self.num_comp, self.P, self.Q, self.quad_mode)
+
+    def apply(self, num_elem, t_mode, eval_mode, u, v, stream=None):
+        if u is not None:
+            _check_dev(u)
+        _check_dev(v)
+        call("fem_b200_basis_apply", self.h, num_elem, int(t_mode), int(eval_mode), _ptr(u),
+             0 if u is None else _n(u), _ptr(v), _n(v), _stream(stream))
+
+
+def mass_build(rx: Restriction, bx: Basis, x, qdata, stream=None) -> None:
+    """qdata ([q][e], device) = det(dx/dX) * w from coordinates x (device)."""
+    _check_dev(x)
+    _check_dev(qdata)
+    call("fem_b200_mass_build", rx.h, bx.h, _ptr(x), _n(x), _ptr(qdata), _n(qdata), _stream(stream))
+
+
+class MassOperator(_Handle):
+    """v = M u, the fused mass operator (its own copy of qdata)."""
+    _destroy = "fem_b200_mass_destroy"
+
+    def __init__(self, ru: Restriction, bu: Basis, qdata, qf=QF.apply_mass):
+        super().__init__()
+        _check_dev(qdata)
+        call("fem_b200_mass_create", ru.h, bu.h, _ptr(qdata), _n(qdata), int(qf), C.addressof(self.h))
+        self.l_size = ru.l_size
+        self.qf = QF(qf)
+
+    def apply(self, u, v, stream=None):
+        _check_dev(u)
+        _check_dev(v)
+        call("fem_b200_mass_apply", self.h, _ptr(u), _n(u), _ptr(v), _n(v), _stream(stream))
+
+    def apply_add(self, u, v, stream=None):
+        _check_dev(u)
+        _check_dev(v)
+        call("fem_b200_mass_apply_add", self.h, _ptr(u), _n(u), _ptr(v), _n(v), _stream(stream))
+
+    def apply_host(self, u: np.ndarray, v: np.ndarray | None = None, stream=None) -> np.ndarray:
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        v = np.empty(self.l_size) if v is None else v
+        call("fem_b200_mass_apply_host", self.h, _ptr(u), u.size, _ptr(v), v.size, _stream(stream))
+        return v
+
+    def info(self):
+        launches, tile = C.c_int(0), C.c_int(0)
+        nbytes = C.c_int64(0)
+        call("fem_b200_mass_info", self.h, C.addressof(launches), C.addressof(tile), C.addressof(nbytes))
+        return {"launches_per_apply": launches.value, "tile_elems": tile.value, "device_bytes": nbytes.value}

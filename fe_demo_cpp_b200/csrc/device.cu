@@ -1,0 +1,714 @@
+// libfem_b200: device objects (restriction, basis, mass plan), kernel
+// dispatch and the extern "C" entry points declared in include/fem_b200.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "common.hpp"
+#include "fem_b200.h"
+#include "host_setup.hpp"
+#include "mass_kernels.cuh"
+#include "restriction_kernels.cuh"
+
+namespace fem_b200 {
+
+thread_local std::string g_last_error;
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+// ---------------------------------------------------------------------------
+// RAII device buffer (move-only), the reference's DeviceArray semantics
+// (include/cuda/device-array.hpp:18-95) without the synchronous copies.
+// ---------------------------------------------------------------------------
+template <class T>
+class DevBuf {
+ public:
+  DevBuf() = default;
+  explicit DevBuf(size_t n) { alloc(n); }
+  ~DevBuf() { release(); }
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : p_(o.p_), n_(o.n_) { o.p_ = nullptr, o.n_ = 0; }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    if (this != &o) {
+      release();
+      p_ = o.p_, n_ = o.n_;
+      o.p_ = nullptr, o.n_ = 0;
+    }
+    return *this;
+  }
+  void alloc(size_t n) {
+    release();
+    if (n == 0) return;
+    FEM_CUDA_CHECK(cudaMalloc(&p_, n * sizeof(T)));
+    n_ = n;
+  }
+  T* get() const { return p_; }
+  size_t size() const { return n_; }
+  size_t bytes() const { return n_ * sizeof(T); }
+
+ private:
+  void release() noexcept {
+    if (p_) (void)cudaFree(p_);
+    p_ = nullptr, n_ = 0;
+  }
+  T* p_ = nullptr;
+  size_t n_ = 0;
+};
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    FEM_CUDA_CHECK(cudaGetDevice(&prev));
+    if (prev != dev) FEM_CUDA_CHECK(cudaSetDevice(dev));
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    if (cudaGetDevice(&cur) == cudaSuccess && cur != prev && prev >= 0) (void)cudaSetDevice(prev);
+  }
+};
+
+inline int current_device() {
+  int d = 0;
+  FEM_CUDA_CHECK(cudaGetDevice(&d));
+  return d;
+}
+
+inline cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
+
+inline int grid_for(int64_t n, int threads) {
+  const int64_t b = (n + threads - 1) / threads;
+  return int(std::max<int64_t>(1, std::min<int64_t>(b, 148LL * 64)));
+}
+
+#define FEM_LAUNCH_CHECK() FEM_CUDA_CHECK(cudaGetLastError())
+
+// ---------------------------------------------------------------------------
+// Restriction
+// ---------------------------------------------------------------------------
+struct RestrictionData {
+  int device = 0;
+  bool strided = false;
+  int num_elem = 0, elem_size = 0, num_comp = 0, comp_stride = 0, l_size = 0;
+  int64_t e_size = 0;
+  int64_t strides[3] = {0, 0, 0};
+  int scatter_mode = FEM_B200_SCATTER_ATOMIC;
+  DevBuf<int> offsets;  // [num_elem][elem_size]
+  int num_nodes = 0;    // transpose map (deterministic offset restrictions)
+  DevBuf<int> l_vec_indices, t_offsets, t_indices;
+};
+
+// ---------------------------------------------------------------------------
+// Basis: host data plus device copies for the generic contraction kernels
+// ---------------------------------------------------------------------------
+struct BasisDev {
+  int device = 0;
+  BasisData h;
+  DevBuf<double> interp, grad, weight;
+  DevBuf<double> scratch;  // ping-pong pass buffers, grown on demand
+  std::mutex scratch_mu;
+};
+
+// ---------------------------------------------------------------------------
+// Mass plan
+// ---------------------------------------------------------------------------
+struct MassPlan;
+using ApplyLauncher = void (*)(const MassPlan&, const double*, double*, double*, cudaStream_t);
+using BuildLauncher = void (*)(const BasisData&, const RestrictionData&, const double*, double*, cudaStream_t);
+
+struct MassPlan {
+  int device = 0;
+  int dim = 0, P = 0, Q = 0, num_comp = 0, comp_run = 0, qf = 0, scatter_mode = 0;
+  int num_elem = 0, l_size = 0, es = 0, nq = 0;
+  int64_t comp_stride = 0;
+  int tile_e = 0;
+  int64_t n_tiles = 0;
+  BasisData basis;
+  std::shared_ptr<RestrictionData> r;
+  DevBuf<int> offs_t;
+  DevBuf<double> qd_t;
+  DevBuf<double> evec;    // deterministic mode: element contributions
+  DevBuf<double> hu, hv;  // staging for the host-memory apply
+  ApplyLauncher launch = nullptr;
+};
+
+template <int P, int Q>
+Mat1D<P, Q> make_mat(const BasisData& b) {
+  Mat1D<P, Q> m;
+  std::memcpy(m.B, b.interp.data(), sizeof(m.B));
+  std::memcpy(m.G, b.grad.data(), sizeof(m.G));
+  std::memcpy(m.W, b.q_weight.data(), sizeof(m.W));
+  return m;
+}
+
+constexpr int kMaxSmemPerCta = 227 * 1024;
+
+// Opt a kernel into more than 48 KB of dynamic shared memory, once per device
+// (the attribute belongs to the device context).
+template <class K>
+void set_smem(K kernel, int bytes, std::atomic<uint64_t>& done) {
+  if (bytes <= 48 * 1024) return;
+  const int dev = current_device();
+  const uint64_t bit = uint64_t(1) << (dev & 63);
+  if (done.load() & bit) return;
+  FEM_CUDA_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  done.fetch_or(bit);
+}
+
+template <int P, int Q>
+void launch_apply3(const MassPlan& p, const double* u, double* v, double* ev, cudaStream_t s) {
+  using L = Mass3D<P, Q>;
+  static std::atomic<uint64_t> smem_set{0};
+  set_smem(mass3d_apply_kernel<P, Q>, L::SMEM, smem_set);
+  mass3d_apply_kernel<P, Q><<<unsigned(p.n_tiles), L::NT, L::SMEM, s>>>(
+      make_mat<P, Q>(p.basis), p.offs_t.get(), p.qd_t.get(), u, v, ev, p.num_elem, p.comp_run, p.comp_stride);
+  FEM_LAUNCH_CHECK();
+}
+
+template <int P, int Q>
+void launch_apply2(const MassPlan& p, const double* u, double* v, double* ev, cudaStream_t s) {
+  using L = Mass2D<P, Q>;
+  static std::atomic<uint64_t> smem_set{0};
+  set_smem(mass2d_apply_kernel<P, Q>, L::SMEM, smem_set);
+  mass2d_apply_kernel<P, Q><<<unsigned(p.n_tiles), L::NT, L::SMEM, s>>>(
+      make_mat<P, Q>(p.basis), p.offs_t.get(), p.qd_t.get(), u, v, ev, p.num_elem, p.comp_run, p.comp_stride);
+  FEM_LAUNCH_CHECK();
+}
+
+template <int P, int Q>
+void launch_apply1(const MassPlan& p, const double* u, double* v, double* ev, cudaStream_t s) {
+  mass1d_apply_kernel<P, Q><<<unsigned(p.n_tiles), 128, 0, s>>>(make_mat<P, Q>(p.basis), p.offs_t.get(),
+                                                                 p.qd_t.get(), u, v, ev, p.num_elem, p.comp_run,
+                                                                 p.comp_stride);
+  FEM_LAUNCH_CHECK();
+}
+
+template <int P, int Q>
+void launch_build3(const BasisData& b, const RestrictionData& r, const double* x, double* qdata, cudaStream_t s) {
+  using L = Build3D<P, Q>;
+  static std::atomic<uint64_t> smem_set{0};
+  set_smem(mass3d_build_kernel<P, Q>, L::SMEM, smem_set);
+  const unsigned grid = unsigned((int64_t(r.num_elem) + L::E - 1) / L::E);
+  mass3d_build_kernel<P, Q><<<grid, L::NT, L::SMEM, s>>>(make_mat<P, Q>(b), r.offsets.get(), x, r.comp_stride, qdata,
+                                                        r.num_elem);
+  FEM_LAUNCH_CHECK();
+}
+
+template <int P, int Q>
+void launch_build2(const BasisData& b, const RestrictionData& r, const double* x, double* qdata, cudaStream_t s) {
+  const unsigned grid = unsigned((int64_t(r.num_elem) + 31) / 32);
+  mass2d_build_kernel<P, Q><<<grid, 32 * Q, 0, s>>>(make_mat<P, Q>(b), r.offsets.get(), x, r.comp_stride, qdata,
+                                                   r.num_elem);
+  FEM_LAUNCH_CHECK();
+}
+
+template <int P, int Q>
+void launch_build1(const BasisData& b, const RestrictionData& r, const double* x, double* qdata, cudaStream_t s) {
+  const unsigned grid = unsigned((int64_t(r.num_elem) + 127) / 128);
+  mass1d_build_kernel<P, Q><<<grid, 128, 0, s>>>(make_mat<P, Q>(b), r.offsets.get(), x, r.comp_stride, qdata,
+                                                r.num_elem);
+  FEM_LAUNCH_CHECK();
+}
+
+// Compiled (P, Q) set: P = 2..8, Q = P .. P+2 (Q = P + 1 is the Gauss rule
+// of the benchmarks; Q = P the collocated GLL case).
+constexpr int kMinP = 2, kMaxP = 8, kQSpan = 3;
+
+template <int P, int DQ>
+struct Table {
+  static void fill(ApplyLauncher (*ap)[kMaxP + 1][kQSpan], BuildLauncher (*bd)[kMaxP + 1][kQSpan]) {
+    constexpr int Q = P + DQ;
+    ap[0][P][DQ] = launch_apply1<P, Q>;
+    ap[1][P][DQ] = launch_apply2<P, Q>;
+    ap[2][P][DQ] = launch_apply3<P, Q>;
+    bd[0][P][DQ] = launch_build1<P, Q>;
+    bd[1][P][DQ] = launch_build2<P, Q>;
+    bd[2][P][DQ] = launch_build3<P, Q>;
+    if constexpr (DQ + 1 < kQSpan)
+      Table<P, DQ + 1>::fill(ap, bd);
+    else if constexpr (P + 1 <= kMaxP)
+      Table<P + 1, 0>::fill(ap, bd);
+  }
+};
+
+struct Dispatch {
+  ApplyLauncher apply[3][kMaxP + 1][kQSpan] = {};
+  BuildLauncher build[3][kMaxP + 1][kQSpan] = {};
+  Dispatch() { Table<kMinP, 0>::fill(apply, build); }
+};
+
+const Dispatch& dispatch() {
+  static Dispatch d;
+  return d;
+}
+
+bool fused_supported(int dim, int P, int Q) {
+  return dim >= 1 && dim <= 3 && P >= kMinP && P <= kMaxP && Q >= P && Q < P + kQSpan;
+}
+
+// Shared memory of the 3D build kernel (5 planes of partial contractions).
+int build3d_smem(int P, int Q) {
+  const int E = 8;
+  return (2 * P * plane_stride(P * Q * E, E) + 3 * P * plane_stride(Q * Q * E, E)) * 8;
+}
+
+std::string shape_str(int dim, int P, int Q) {
+  return "dim=" + std::to_string(dim) + ", P=" + std::to_string(P) + ", Q=" + std::to_string(Q);
+}
+
+}  // namespace fem_b200
+
+using namespace fem_b200;
+
+struct fem_b200_restriction_s {
+  std::shared_ptr<RestrictionData> d;
+};
+struct fem_b200_basis_s {
+  std::unique_ptr<BasisDev> d;
+};
+struct fem_b200_mass_s {
+  std::unique_ptr<MassPlan> d;
+};
+
+// ===========================================================================
+// extern "C" entry points
+// ===========================================================================
+extern "C" {
+
+const char* fem_b200_last_error(void) { return g_last_error.c_str(); }
+
+int fem_b200_version(void) { return 100; }
+
+int fem_b200_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+// ---- host set-up ----------------------------------------------------------
+int fem_b200_gauss_legendre(int Q, double* x, double* w) {
+  return guarded([&] {
+    require(x && w, "gauss_legendre_quadrature: NULL output");
+    gauss_legendre(Q, x, w);
+  });
+}
+
+int fem_b200_gauss_lobatto(int Q, double* x, double* w) {
+  return guarded([&] {
+    require(x != nullptr, "gauss_lobatto_points: NULL output");
+    gauss_lobatto(Q, x, w);
+  });
+}
+
+int fem_b200_lagrange_basis_matrix(int P, const double* nodes, int M, const double* pts, double* interp,
+                                   double* grad) {
+  return guarded([&] {
+    require(P >= 1 && M >= 0 && nodes && (M == 0 || (pts && interp && grad)), "lagrange_basis_matrix: bad arguments");
+    lagrange_matrices(P, nodes, M, pts, interp, grad);
+  });
+}
+
+int fem_b200_tensor_h1_lagrange(int dim, int num_comp, int P, int Q, int quad_mode, double* q_ref, double* q_weight,
+                                double* interp, double* grad) {
+  return guarded([&] {
+    BasisData b = make_basis(dim, num_comp, P, Q, quad_mode);
+    if (q_ref) std::copy(b.q_ref.begin(), b.q_ref.end(), q_ref);
+    if (q_weight) std::copy(b.q_weight.begin(), b.q_weight.end(), q_weight);
+    if (interp) std::copy(b.interp.begin(), b.interp.end(), interp);
+    if (grad) std::copy(b.grad.begin(), b.grad.end(), grad);
+  });
+}
+
+int fem_b200_restriction_check_offset(int num_elem, int elem_size, int num_comp, int comp_stride, int l_size,
+                                      const int* offsets, int64_t n_offsets) {
+  return guarded([&] { check_offset(num_elem, elem_size, num_comp, comp_stride, l_size, offsets, n_offsets); });
+}
+
+int fem_b200_restriction_check_strided(int num_elem, int elem_size, int num_comp, int l_size, const int* strides) {
+  return guarded([&] { check_strided(num_elem, elem_size, num_comp, l_size, strides); });
+}
+
+int fem_b200_transpose_map(int num_elem, int elem_size, int l_size, const int* offsets, int* l_vec_indices,
+                           int* t_offsets, int* t_indices, int* num_nodes) {
+  return guarded([&] {
+    require(num_elem > 0 && elem_size > 0 && l_size > 0 && offsets && l_vec_indices && t_offsets && t_indices,
+            "build_transpose_map: bad arguments");
+    for (int64_t t = 0; t < int64_t(num_elem) * elem_size; ++t)
+      require(offsets[t] >= 0 && offsets[t] < l_size, "build_transpose_map: offset out of range");
+    const int n = transpose_map(num_elem, elem_size, l_size, offsets, l_vec_indices, t_offsets, t_indices);
+    if (num_nodes) *num_nodes = n;
+  });
+}
+
+// ---- restriction ------------------------------------------------------------
+int fem_b200_restriction_create_offset(int num_elem, int elem_size, int num_comp, int comp_stride, int l_size,
+                                       const int* offsets, int scatter_mode, fem_b200_restriction* out) {
+  return guarded([&] {
+    require(out != nullptr, "elem_restriction_create: NULL output handle");
+    require(scatter_mode == FEM_B200_SCATTER_ATOMIC || scatter_mode == FEM_B200_SCATTER_DETERMINISTIC,
+            "elem_restriction_create: unknown scatter mode");
+    const int64_t n_t = int64_t(num_elem) * elem_size;
+    check_offset(num_elem, elem_size, num_comp, comp_stride, l_size, offsets, n_t);
+    auto d = std::make_shared<RestrictionData>();
+    d->device = current_device();
+    d->num_elem = num_elem, d->elem_size = elem_size, d->num_comp = num_comp;
+    d->comp_stride = comp_stride;
+    d->l_size = l_size;
+    d->e_size = int64_t(num_comp) * n_t;
+    d->scatter_mode = scatter_mode;
+    d->offsets.alloc(size_t(n_t));
+    FEM_CUDA_CHECK(cudaMemcpy(d->offsets.get(), offsets, n_t * sizeof(int), cudaMemcpyHostToDevice));
+    if (scatter_mode == FEM_B200_SCATTER_DETERMINISTIC) {
+      std::vector<int> lvi(static_cast<size_t>(l_size)), toff(static_cast<size_t>(l_size) + 1),
+          tidx(static_cast<size_t>(n_t));
+      const int n = transpose_map(num_elem, elem_size, l_size, offsets, lvi.data(), toff.data(), tidx.data());
+      d->num_nodes = n;
+      d->l_vec_indices.alloc(size_t(n));
+      d->t_offsets.alloc(size_t(n) + 1);
+      d->t_indices.alloc(size_t(n_t));
+      FEM_CUDA_CHECK(cudaMemcpy(d->l_vec_indices.get(), lvi.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+      FEM_CUDA_CHECK(cudaMemcpy(d->t_offsets.get(), toff.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice));
+      FEM_CUDA_CHECK(cudaMemcpy(d->t_indices.get(), tidx.data(), n_t * sizeof(int), cudaMemcpyHostToDevice));
+    }
+    *out = new fem_b200_restriction_s{std::move(d)};
+  });
+}
+
+int fem_b200_restriction_create_strided(int num_elem, int elem_size, int num_comp, int l_size, const int* strides,
+                                        fem_b200_restriction* out) {
+  return guarded([&] {
+    require(out != nullptr, "elem_restriction_create_strided: NULL output handle");
+    check_strided(num_elem, elem_size, num_comp, l_size, strides);
+    auto d = std::make_shared<RestrictionData>();
+    d->device = current_device();
+    d->strided = true;
+    d->num_elem = num_elem, d->elem_size = elem_size, d->num_comp = num_comp, d->l_size = l_size;
+    d->e_size = int64_t(num_comp) * elem_size * num_elem;
+    if (strides) {
+      for (int i = 0; i < 3; ++i) d->strides[i] = strides[i];
+    } else {
+      d->strides[0] = num_elem, d->strides[1] = int64_t(elem_size) * num_elem, d->strides[2] = 1;
+    }
+    *out = new fem_b200_restriction_s{std::move(d)};
+  });
+}
+
+int fem_b200_restriction_destroy(fem_b200_restriction r) {
+  return guarded([&] { delete r; });
+}
+
+int fem_b200_restriction_sizes(fem_b200_restriction r, int* num_elem, int* elem_size, int* num_comp, int* l_size,
+                               int64_t* e_size) {
+  return guarded([&] {
+    require(r && r->d, "restriction: NULL handle");
+    const RestrictionData& d = *r->d;
+    if (num_elem) *num_elem = d.num_elem;
+    if (elem_size) *elem_size = d.elem_size;
+    if (num_comp) *num_comp = d.num_comp;
+    if (l_size) *l_size = d.l_size;
+    if (e_size) *e_size = d.e_size;
+  });
+}
+
+int fem_b200_restriction_transpose_map(fem_b200_restriction r, int* l_vec_indices, int* t_offsets, int* t_indices,
+                                       int* num_nodes) {
+  return guarded([&] {
+    require(r && r->d, "restriction: NULL handle");
+    const RestrictionData& d = *r->d;
+    require(!d.strided && d.scatter_mode == FEM_B200_SCATTER_DETERMINISTIC,
+            "restriction has no transpose map (deterministic offset restrictions only)");
+    DeviceGuard g(d.device);
+    if (num_nodes) *num_nodes = d.num_nodes;
+    const int64_t n_t = int64_t(d.num_elem) * d.elem_size;
+    if (l_vec_indices)
+      FEM_CUDA_CHECK(cudaMemcpy(l_vec_indices, d.l_vec_indices.get(), d.num_nodes * sizeof(int), cudaMemcpyDeviceToHost));
+    if (t_offsets)
+      FEM_CUDA_CHECK(cudaMemcpy(t_offsets, d.t_offsets.get(), (d.num_nodes + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+    if (t_indices) FEM_CUDA_CHECK(cudaMemcpy(t_indices, d.t_indices.get(), n_t * sizeof(int), cudaMemcpyDeviceToHost));
+  });
+}
+
+int fem_b200_restriction_apply(fem_b200_restriction r, int t_mode, const double* in, int64_t n_in, double* out,
+                               int64_t n_out, void* stream) {
+  return guarded([&] {
+    require(r && r->d, "elem_restriction_apply: NULL handle");
+    const RestrictionData& d = *r->d;
+    const bool tr = t_mode == FEM_B200_TRANSPOSE;
+    require(t_mode == FEM_B200_NOTRANSPOSE || tr, "elem_restriction_apply: unknown t_mode");
+    require(n_in == (tr ? d.e_size : d.l_size), "elem_restriction_apply: in has the wrong size");
+    require(n_out == (tr ? int64_t(d.l_size) : d.e_size),
+            tr ? "elem_restriction_apply: Transpose adds into out, which must already have l_size entries"
+               : "elem_restriction_apply: out must have e_size entries");
+    require(in && out, "elem_restriction_apply: NULL array");
+    DeviceGuard g(d.device);
+    cudaStream_t s = as_stream(stream);
+    if (d.strided) {
+      const int grid = grid_for(d.e_size, 256);
+      if (!tr)
+        strided_kernel<0><<<grid, 256, 0, s>>>(d.num_elem, d.elem_size, d.num_comp, d.strides[0], d.strides[1],
+                                               d.strides[2], in, out);
+      else
+        strided_kernel<1><<<grid, 256, 0, s>>>(d.num_elem, d.elem_size, d.num_comp, d.strides[0], d.strides[1],
+                                               d.strides[2], in, out);
+    } else if (!tr || d.scatter_mode == FEM_B200_SCATTER_ATOMIC) {
+      const dim3 grid(unsigned((d.elem_size + kTile - 1) / kTile), unsigned((d.num_elem + kTile - 1) / kTile));
+      const dim3 block(kTile, 8);
+      if (!tr)
+        offset_tile_kernel<0><<<grid, block, 0, s>>>(d.offsets.get(), d.num_elem, d.elem_size, d.num_comp,
+                                                     d.comp_stride, in, out);
+      else
+        offset_tile_kernel<1><<<grid, block, 0, s>>>(d.offsets.get(), d.num_elem, d.elem_size, d.num_comp,
+                                                     d.comp_stride, in, out);
+    } else {
+      csr_scatter_kernel<<<grid_for(d.num_nodes, 256), 256, 0, s>>>(
+          d.num_nodes, d.num_elem, d.elem_size, d.num_comp, d.comp_stride, d.l_vec_indices.get(), d.t_offsets.get(),
+          d.t_indices.get(), in, out);
+    }
+    FEM_LAUNCH_CHECK();
+  });
+}
+
+int fem_b200_restriction_multiplicity(fem_b200_restriction r, double* mult, int64_t n, void* stream) {
+  return guarded([&] {
+    require(r && r->d, "elem_restriction_get_multiplicity: NULL handle");
+    const RestrictionData& d = *r->d;
+    require(n == d.l_size && mult, "elem_restriction_get_multiplicity: mult must have l_size entries");
+    DeviceGuard g(d.device);
+    cudaStream_t s = as_stream(stream);
+    FEM_CUDA_CHECK(cudaMemsetAsync(mult, 0, n * sizeof(double), s));
+    if (d.strided) {
+      // every strided index is hit once: scatter a vector of ones
+      DevBuf<double> ones(size_t(d.e_size));
+      std::vector<double> h(size_t(d.e_size), 1.0);
+      FEM_CUDA_CHECK(cudaMemcpyAsync(ones.get(), h.data(), d.e_size * sizeof(double), cudaMemcpyHostToDevice, s));
+      strided_kernel<1><<<grid_for(d.e_size, 256), 256, 0, s>>>(d.num_elem, d.elem_size, d.num_comp, d.strides[0],
+                                                                 d.strides[1], d.strides[2], ones.get(), mult);
+      FEM_LAUNCH_CHECK();
+      FEM_CUDA_CHECK(cudaStreamSynchronize(s));
+      return;
+    }
+    const dim3 grid(unsigned((d.elem_size + kTile - 1) / kTile), unsigned((d.num_elem + kTile - 1) / kTile));
+    offset_tile_kernel<2><<<grid, dim3(kTile, 8), 0, s>>>(d.offsets.get(), d.num_elem, d.elem_size, d.num_comp,
+                                                          d.comp_stride, nullptr, mult);
+    FEM_LAUNCH_CHECK();
+  });
+}
+
+// ---- basis --------------------------------------------------------------------
+int fem_b200_basis_create(int dim, int num_comp, int P, int Q, int quad_mode, fem_b200_basis* out) {
+  return guarded([&] {
+    require(out != nullptr, "create_tensor_H1_lagrange: NULL output handle");
+    auto d = std::make_unique<BasisDev>();
+    d->h = make_basis(dim, num_comp, P, Q, quad_mode);
+    d->device = current_device();
+    d->interp.alloc(d->h.interp.size());
+    d->grad.alloc(d->h.grad.size());
+    d->weight.alloc(d->h.q_weight.size());
+    FEM_CUDA_CHECK(cudaMemcpy(d->interp.get(), d->h.interp.data(), d->interp.bytes(), cudaMemcpyHostToDevice));
+    FEM_CUDA_CHECK(cudaMemcpy(d->grad.get(), d->h.grad.data(), d->grad.bytes(), cudaMemcpyHostToDevice));
+    FEM_CUDA_CHECK(cudaMemcpy(d->weight.get(), d->h.q_weight.data(), d->weight.bytes(), cudaMemcpyHostToDevice));
+    *out = new fem_b200_basis_s{std::move(d)};
+  });
+}
+
+int fem_b200_basis_destroy(fem_b200_basis b) {
+  return guarded([&] { delete b; });
+}
+
+int fem_b200_basis_apply(fem_b200_basis b, int num_elem, int t_mode, int eval_mode, const double* u, int64_t n_u,
+                         double* v, int64_t n_v, void* stream) {
+  return guarded([&] {
+    require(b && b->d, "tensor_basis_apply: NULL handle");
+    BasisDev& bd = *b->d;
+    const BasisData& h = bd.h;
+    const bool tr = t_mode == FEM_B200_TRANSPOSE;
+    require(t_mode == FEM_B200_NOTRANSPOSE || tr, "tensor_basis_apply: unknown t_mode");
+    require(num_elem > 0, "tensor_basis_apply: num_elem must be positive");
+    const int64_t pn = ipow(h.P, h.dim) * h.num_comp * num_elem;  // nodal size
+    const int64_t qn = ipow(h.Q, h.dim) * h.num_comp * num_elem;  // one block at the points
+    DeviceGuard g(bd.device);
+    cudaStream_t s = as_stream(stream);
+    if (eval_mode == FEM_B200_EVAL_WEIGHT) {
+      require(!tr, "EvalMode::Weight is incompatible with ContractMode::Transpose");
+      require(n_v == ipow(h.Q, h.dim) * num_elem && v, "tensor_basis_apply: v has the wrong size");
+      weight_kernel<<<grid_for(n_v, 256), 256, 0, s>>>(h.dim, h.Q, bd.weight.get(), num_elem, v);
+      FEM_LAUNCH_CHECK();
+      return;
+    }
+    require(eval_mode == FEM_B200_EVAL_INTERP || eval_mode == FEM_B200_EVAL_GRAD,
+            "tensor_basis_apply: unknown eval_mode");
+    const bool grad = eval_mode == FEM_B200_EVAL_GRAD;
+    const int64_t in_n = tr ? (grad ? h.dim * qn : qn) : pn;
+    const int64_t out_n = tr ? pn : (grad ? h.dim * qn : qn);
+    require(n_u == in_n && u, "tensor_basis_apply: u has the wrong size");
+    require(n_v == out_n && v, "tensor_basis_apply: v has the wrong size");
+    const int P = tr ? h.Q : h.P, Q = tr ? h.P : h.Q;  // contracted in / out sizes
+    const int64_t big = h.num_comp * ipow(std::max(h.P, h.Q), h.dim) * num_elem;
+    std::lock_guard<std::mutex> lock(bd.scratch_mu);
+    if (h.dim > 1 && bd.scratch.size() < size_t(2 * big)) bd.scratch.alloc(size_t(2 * big));
+    double* tmp[2] = {bd.scratch.get(), bd.scratch.get() + big};
+    const int naxes = grad ? h.dim : 1;
+    for (int ax = 0; ax < naxes; ++ax) {
+      int64_t pre = h.num_comp * ipow(P, h.dim - 1), post = num_elem;
+      for (int dd = 0; dd < h.dim; ++dd) {
+        const double* mat = (grad && dd == ax) ? bd.grad.get() : bd.interp.get();
+        const double* src = dd == 0 ? (tr && grad ? u + ax * qn : u) : tmp[dd % 2];
+        const bool last = dd == h.dim - 1;
+        double* dst = last ? (tr ? v : (grad ? v + ax * qn : v)) : tmp[(dd + 1) % 2];
+        const int add = (last && tr && grad && ax > 0) ? 1 : 0;
+        const int64_t n = pre * Q * post;
+        contract_kernel<<<grid_for(n, 256), 256, 0, s>>>(pre, P, post, Q, mat, tr ? 1 : 0, add, src, dst);
+        FEM_LAUNCH_CHECK();
+        pre /= P;
+        post *= Q;
+      }
+    }
+  });
+}
+
+// ---- mass ---------------------------------------------------------------------
+int fem_b200_mass_build(fem_b200_restriction rx, fem_b200_basis bx, const double* x, int64_t n_x, double* qdata,
+                        int64_t n_qdata, void* stream) {
+  return guarded([&] {
+    require(rx && rx->d && bx && bx->d, "mass build: NULL handle");
+    const RestrictionData& r = *rx->d;
+    const BasisData& b = bx->d->h;
+    require(!r.strided, "mass build: the coordinate restriction must be an offset restriction");
+    require(b.num_comp == b.dim && r.num_comp == b.dim, "mass build: coordinates need num_comp == dim");
+    require(r.elem_size == ipow(b.P, b.dim), "operator_set_field 'dx': restriction elem_size must equal basis P_1d^dim");
+    require(n_x == r.l_size && x, "mass build: x must have l_size entries");
+    require(n_qdata == ipow(b.Q, b.dim) * r.num_elem && qdata, "mass build: qdata must have Q^dim*num_elem entries");
+    if (!fused_supported(b.dim, b.P, b.Q) || (b.dim == 3 && build3d_smem(b.P, b.Q) > kMaxSmemPerCta))
+      throw unsupported_error("mass build: no device kernel for " + shape_str(b.dim, b.P, b.Q) +
+                              " (P in 2..8, Q in P..P+2; dim 3 with P = 8 up to Q = 9)");
+    DeviceGuard g(r.device);
+    dispatch().build[b.dim - 1][b.P][b.Q - b.P](b, r, x, qdata, as_stream(stream));
+  });
+}
+
+int fem_b200_mass_create(fem_b200_restriction ru, fem_b200_basis bu, const double* qdata, int64_t n_qdata, int qf,
+                         fem_b200_mass* out) {
+  return guarded([&] {
+    require(out != nullptr, "operator_create: NULL output handle");
+    require(ru && ru->d && bu && bu->d, "operator_set_field: NULL handle");
+    const std::shared_ptr<RestrictionData>& r = ru->d;
+    const BasisData& b = bu->d->h;
+    require(qf == FEM_B200_QF_APPLY_MASS || qf == FEM_B200_QF_APPLY_MASS_VECTOR, "operator_create: unknown QFunction");
+    require(!r->strided, "operator_set_field 'u': the active field needs an offset restriction");
+    require(r->num_comp == b.num_comp, "operator_set_field 'u': restriction and basis num_comp differ");
+    require(r->elem_size == ipow(b.P, b.dim), "operator_set_field 'u': restriction elem_size must equal basis P_1d^dim");
+    const int64_t nq = ipow(b.Q, b.dim);
+    require(n_qdata == nq * r->num_elem && qdata, "operator_set_field 'qdata': passive vector size must equal restriction l_size");
+    if (!fused_supported(b.dim, b.P, b.Q))
+      throw unsupported_error("operator_apply: no fused device kernel for " + shape_str(b.dim, b.P, b.Q) +
+                              " (P in 2..8, Q in P..P+2)");
+    auto p = std::make_unique<MassPlan>();
+    p->device = r->device;
+    DeviceGuard g(p->device);
+    p->dim = b.dim, p->P = b.P, p->Q = b.Q, p->num_comp = b.num_comp;
+    p->qf = qf;
+    p->comp_run = qf == FEM_B200_QF_APPLY_MASS ? 1 : b.num_comp;
+    p->scatter_mode = r->scatter_mode;
+    p->num_elem = r->num_elem, p->l_size = r->l_size, p->es = r->elem_size, p->nq = int(nq);
+    p->comp_stride = r->comp_stride;
+    p->basis = b;
+    p->r = r;
+    p->tile_e = b.dim == 3 ? 8 : (b.dim == 2 ? 32 : 128);
+    p->n_tiles = (int64_t(p->num_elem) + p->tile_e - 1) / p->tile_e;
+    const int64_t ne_pad = p->n_tiles * p->tile_e;
+    p->offs_t.alloc(size_t(ne_pad * p->es));
+    p->qd_t.alloc(size_t(ne_pad * p->nq));
+    tile_offsets_kernel<<<grid_for(ne_pad * p->es, 256), 256>>>(r->offsets.get(), p->num_elem, p->es, p->tile_e,
+                                                                ne_pad * p->es, p->offs_t.get());
+    FEM_LAUNCH_CHECK();
+    tile_qdata_kernel<<<grid_for(ne_pad * p->nq, 256), 256>>>(qdata, p->num_elem, p->Q, p->nq, p->tile_e,
+                                                              ne_pad * p->nq, p->qd_t.get());
+    FEM_LAUNCH_CHECK();
+    if (p->scatter_mode == FEM_B200_SCATTER_DETERMINISTIC) p->evec.alloc(size_t(int64_t(p->comp_run) * p->es * p->num_elem));
+    p->launch = dispatch().apply[b.dim - 1][b.P][b.Q - b.P];
+    FEM_CUDA_CHECK(cudaDeviceSynchronize());
+    *out = new fem_b200_mass_s{std::move(p)};
+  });
+}
+
+int fem_b200_mass_destroy(fem_b200_mass op) {
+  return guarded([&] { delete op; });
+}
+
+namespace {
+void mass_apply_impl(MassPlan& p, const double* u, double* v, bool zero, cudaStream_t s) {
+  if (zero) FEM_CUDA_CHECK(cudaMemsetAsync(v, 0, size_t(p.l_size) * sizeof(double), s));
+  if (p.scatter_mode == FEM_B200_SCATTER_ATOMIC) {
+    p.launch(p, u, v, nullptr, s);
+    return;
+  }
+  const RestrictionData& r = *p.r;
+  p.launch(p, u, v, p.evec.get(), s);
+  csr_scatter_kernel<<<grid_for(r.num_nodes, 256), 256, 0, s>>>(r.num_nodes, p.num_elem, p.es, p.comp_run,
+                                                                p.comp_stride, r.l_vec_indices.get(),
+                                                                r.t_offsets.get(), r.t_indices.get(), p.evec.get(), v);
+  FEM_LAUNCH_CHECK();
+}
+}  // namespace
+
+int fem_b200_mass_apply(fem_b200_mass op, const double* u, int64_t n_u, double* v, int64_t n_v, void* stream) {
+  return guarded([&] {
+    require(op && op->d, "operator_apply: NULL handle");
+    MassPlan& p = *op->d;
+    require(n_u == p.l_size && u, "operator_apply: input vector size does not match active_in_l_size");
+    require(n_v == p.l_size && v, "operator_apply: output vector size does not match active_out_l_size");
+    DeviceGuard g(p.device);
+    mass_apply_impl(p, u, v, true, as_stream(stream));
+  });
+}
+
+int fem_b200_mass_apply_add(fem_b200_mass op, const double* u, int64_t n_u, double* v, int64_t n_v, void* stream) {
+  return guarded([&] {
+    require(op && op->d, "operator_apply: NULL handle");
+    MassPlan& p = *op->d;
+    require(n_u == p.l_size && u, "operator_apply: input vector size does not match active_in_l_size");
+    require(n_v == p.l_size && v, "operator_apply: output vector size does not match active_out_l_size");
+    DeviceGuard g(p.device);
+    mass_apply_impl(p, u, v, false, as_stream(stream));
+  });
+}
+
+int fem_b200_mass_apply_host(fem_b200_mass op, const double* u_host, int64_t n_u, double* v_host, int64_t n_v,
+                             void* stream) {
+  return guarded([&] {
+    require(op && op->d, "operator_apply: NULL handle");
+    MassPlan& p = *op->d;
+    require(n_u == p.l_size && u_host, "operator_apply: input vector size does not match active_in_l_size");
+    require(n_v == p.l_size && v_host, "operator_apply: output vector size does not match active_out_l_size");
+    DeviceGuard g(p.device);
+    cudaStream_t s = as_stream(stream);
+    if (p.hu.size() != size_t(p.l_size)) p.hu.alloc(size_t(p.l_size));
+    if (p.hv.size() != size_t(p.l_size)) p.hv.alloc(size_t(p.l_size));
+    const size_t bytes = size_t(p.l_size) * sizeof(double);
+    FEM_CUDA_CHECK(cudaMemcpyAsync(p.hu.get(), u_host, bytes, cudaMemcpyHostToDevice, s));
+    mass_apply_impl(p, p.hu.get(), p.hv.get(), true, s);
+    FEM_CUDA_CHECK(cudaMemcpyAsync(v_host, p.hv.get(), bytes, cudaMemcpyDeviceToHost, s));
+    FEM_CUDA_CHECK(cudaStreamSynchronize(s));
+  });
+}
+
+int fem_b200_mass_info(fem_b200_mass op, int* launches_per_apply, int* tile_elems, int64_t* device_bytes) {
+  return guarded([&] {
+    require(op && op->d, "mass info: NULL handle");
+    const MassPlan& p = *op->d;
+    if (launches_per_apply) *launches_per_apply = p.scatter_mode == FEM_B200_SCATTER_ATOMIC ? 1 : 2;
+    if (tile_elems) *tile_elems = p.tile_e;
+    if (device_bytes)
+      *device_bytes = int64_t(p.offs_t.bytes() + p.qd_t.bytes() + p.evec.bytes() + p.hu.bytes() + p.hv.bytes());
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,564 @@
+// Fused sm_100a kernels of the mass operator and its geometric-factor build.
+//
+// One CTA owns a tile of E consecutive elements.  Lanes run over the tile's
+// elements fastest (thread t -> element t % E, "column" t / E), so every
+// global stream of the path -- offsets, the L-vector gather, qdata, the
+// E-vector -- is read or written by consecutive lanes at consecutive element
+// indices, the element-innermost layout of the reference
+// (include/elem-restriction.hpp:49-51).  For dim = 3 a thread owns one
+// column along the last axis in registers; the contractions along the other
+// axes exchange through shared memory, padded so that a half-warp never has a
+// bank conflict.  The 1D matrices live in the kernel's parameter bank
+// (__grid_constant__), so each FMA reads its matrix entry as a constant
+// operand: no shared-memory or register traffic for B or G.
+//
+// Algorithm (per element): the reference's operator_apply on the mass
+// QFunction (src/operator.cpp:148-182): gather (src/elem-restriction.cpp:64-72),
+// dim contractions with interp_1d (src/tensor-contract.cpp:74-91),
+// v = qdata * u (include/qfunctions/mass.hpp:45-51), the transposed
+// contractions, scatter-add (src/elem-restriction.cpp:73-82).  The axis order
+// of the contractions differs (z first here, x first there), so results agree
+// with the reference to rounding, not bitwise.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace fem_b200 {
+
+template <int P, int Q>
+struct Mat1D {
+  double B[Q * P];  // interp_1d, row-major [q][p]
+  double G[Q * P];  // grad_1d
+  double W[Q];      // q_weight_1d
+};
+
+// Shared-memory plane stride for a tile of 8 elements: an odd multiple of 8
+// doubles, so two adjacent columns of a half-warp land 8 doubles (16 banks)
+// apart.  Tiles of >= 16 elements need no padding (a half-warp is one column).
+__host__ __device__ constexpr int plane_stride(int n, int E) {
+  return (E >= 16 || (n / 8) % 2 == 1) ? n : n + 8;
+}
+__host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
+
+// ---------------------------------------------------------------------------
+// Tiled layouts owned by a mass plan (built once at create time)
+//   offsets  [tile][i][e]           i = local node (x fastest)
+//   qdata    [tile][qx][col][e]     col = q / Q  (the other axes), q = qx + Q*col
+// Elements past num_elem are padding (offset 0, qdata 0) and never scattered.
+// ---------------------------------------------------------------------------
+__global__ void tile_offsets_kernel(const int* __restrict__ offsets, int num_elem, int elem_size, int E,
+                                    int64_t n_out, int* __restrict__ out) {
+  for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < n_out; t += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t el = t % E, rest = t / E;
+    const int64_t i = rest % elem_size, tile = rest / elem_size;
+    const int64_t e = tile * E + el;
+    out[t] = e < num_elem ? offsets[e * elem_size + i] : 0;
+  }
+}
+
+__global__ void tile_qdata_kernel(const double* __restrict__ qdata, int num_elem, int Q, int nq, int E, int64_t n_out,
+                                  double* __restrict__ out) {
+  const int ncol = nq / Q;
+  for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < n_out; t += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t el = t % E, rest = t / E;
+    const int64_t col = rest % ncol, rest2 = rest / ncol;
+    const int64_t qx = rest2 % Q, tile = rest2 / Q;
+    const int64_t e = tile * E + el;
+    const int64_t q = qx + Q * col;
+    out[t] = e < num_elem ? qdata[q * num_elem + e] : 0.0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// dim = 3 fused apply.  E = 8 elements, 8*Q*Q threads.
+//   phase A  (px,py):  gather z-column, contract z          -> S1
+//   phase B  (px,qz):  contract y                            -> S2
+//   phase C  (qy,qz):  contract x, times qdata, contract x^T -> S3
+//   phase F  (px,qz):  contract y^T                          -> S4
+//   phase G  (px,py):  contract z^T, scatter-add (or E-vector store)
+// S1, S3 share buffer A and S2, S4 buffer B; each array is laid out so its
+// reader's columns are contiguous, and its planes are padded (plane_stride).
+// ---------------------------------------------------------------------------
+template <int P, int Q>
+struct Mass3D {
+  static constexpr int E = 8;
+  static constexpr int NT = E * Q * Q;
+  static constexpr int PS1 = plane_stride(P * Q * E, E);  // S1[py][qz*P+px][e]
+  static constexpr int PS2 = plane_stride(Q * Q * E, E);  // S2[px][qz*Q+qy][e]
+  static constexpr int PS3 = plane_stride(P * Q * E, E);  // S3[qy][qz*P+px][e]
+  static constexpr int PS4 = plane_stride(P * P * E, E);  // S4[qz][py*P+px][e]
+  static constexpr int SA = cmax(P * PS1, Q * PS3);
+  static constexpr int SB = cmax(P * PS2, Q * PS4);
+  static constexpr int SMEM = (SA + SB) * 8;
+  static constexpr int ES = P * P * P, NQ = Q * Q * Q;
+};
+
+// num_comp_run components are processed (1 for the reference apply_mass,
+// which only touches component 0); component k reads/writes at + k*comp_stride.
+// ev == nullptr: atomic scatter-add into v.  ev != nullptr: the element
+// contributions are stored in the E-vector layout [k][i][e] (deterministic
+// mode; a transpose-map reduction follows).
+template <int P, int Q>
+__global__ void __launch_bounds__(Mass3D<P, Q>::NT) mass3d_apply_kernel(
+    const __grid_constant__ Mat1D<P, Q> m, const int* __restrict__ offs, const double* __restrict__ qd,
+    const double* __restrict__ u, double* __restrict__ v, double* __restrict__ ev, int num_elem, int num_comp_run,
+    int64_t comp_stride) {
+  using L = Mass3D<P, Q>;
+  constexpr int E = L::E;
+  extern __shared__ double smem[];
+  double* sa = smem;
+  double* sb = smem + L::SA;
+  const int t = threadIdx.x, e = t % E, col = t / E;
+  const int64_t tile = blockIdx.x;
+  const int64_t eg = tile * E + e;
+  const bool valid = eg < num_elem;
+  const bool nodal = col < P * P;  // (px, py) = (col % P, col / P)
+  const bool mixed = col < P * Q;  // (px, qz) = (col % P, col / P)
+
+  // Prefetch: this thread's qdata row (qy, qz) = (col % Q, col / Q), all qx.
+  double qv[Q];
+  {
+    const double* qt = qd + tile * (int64_t(L::NQ) * E) + col * E + e;
+#pragma unroll
+    for (int qx = 0; qx < Q; ++qx) qv[qx] = __ldg(qt + qx * (Q * Q * E));
+  }
+  int off[P];
+  if (nodal) {
+    const int* ot = offs + tile * (int64_t(L::ES) * E) + col * E + e;
+#pragma unroll
+    for (int pz = 0; pz < P; ++pz) off[pz] = __ldg(ot + pz * (P * P * E));
+  }
+
+  for (int k = 0; k < num_comp_run; ++k) {
+    const int64_t ks = k * comp_stride;
+    if (nodal) {  // phase A
+      double x[P];
+#pragma unroll
+      for (int pz = 0; pz < P; ++pz) x[pz] = __ldg(u + off[pz] + ks);
+      const int px = col % P, py = col / P;
+#pragma unroll
+      for (int qz = 0; qz < Q; ++qz) {
+        double s = 0.0;
+#pragma unroll
+        for (int pz = 0; pz < P; ++pz) s += m.B[qz * P + pz] * x[pz];
+        sa[py * L::PS1 + (qz * P + px) * E + e] = s;
+      }
+    }
+    __syncthreads();
+    if (mixed) {  // phase B
+      double y[P];
+#pragma unroll
+      for (int py = 0; py < P; ++py) y[py] = sa[py * L::PS1 + col * E + e];
+      const int px = col % P, qz = col / P;
+#pragma unroll
+      for (int qy = 0; qy < Q; ++qy) {
+        double s = 0.0;
+#pragma unroll
+        for (int py = 0; py < P; ++py) s += m.B[qy * P + py] * y[py];
+        sb[px * L::PS2 + (qz * Q + qy) * E + e] = s;
+      }
+    }
+    __syncthreads();
+    {  // phase C: x, pointwise mass, x^T
+      double w[P];
+#pragma unroll
+      for (int px = 0; px < P; ++px) w[px] = sb[px * L::PS2 + col * E + e];
+      double r[Q];
+#pragma unroll
+      for (int qx = 0; qx < Q; ++qx) {
+        double s = 0.0;
+#pragma unroll
+        for (int px = 0; px < P; ++px) s += m.B[qx * P + px] * w[px];
+        r[qx] = qv[qx] * s;
+      }
+      const int qy = col % Q, qz = col / Q;
+#pragma unroll
+      for (int px = 0; px < P; ++px) {
+        double s = 0.0;
+#pragma unroll
+        for (int qx = 0; qx < Q; ++qx) s += m.B[qx * P + px] * r[qx];
+        sa[qy * L::PS3 + (qz * P + px) * E + e] = s;
+      }
+    }
+    __syncthreads();
+    if (mixed) {  // phase F: y^T
+      double y[Q];
+#pragma unroll
+      for (int qy = 0; qy < Q; ++qy) y[qy] = sa[qy * L::PS3 + col * E + e];
+      const int px = col % P, qz = col / P;
+#pragma unroll
+      for (int py = 0; py < P; ++py) {
+        double s = 0.0;
+#pragma unroll
+        for (int qy = 0; qy < Q; ++qy) s += m.B[qy * P + py] * y[qy];
+        sb[qz * L::PS4 + (py * P + px) * E + e] = s;
+      }
+    }
+    __syncthreads();
+    if (nodal) {  // phase G: z^T and the scatter
+      double z[Q];
+#pragma unroll
+      for (int qz = 0; qz < Q; ++qz) z[qz] = sb[qz * L::PS4 + col * E + e];
+#pragma unroll
+      for (int pz = 0; pz < P; ++pz) {
+        double s = 0.0;
+#pragma unroll
+        for (int qz = 0; qz < Q; ++qz) s += m.B[qz * P + pz] * z[qz];
+        if (valid) {
+          if (ev)
+            ev[(int64_t(k) * L::ES + pz * P * P + col) * num_elem + eg] = s;
+          else
+            atomicAdd(v + off[pz] + ks, s);
+        }
+      }
+    }
+    // The next component's phase A writes buffer A, whose last readers
+    // (phase F) finished before the barrier above; its phase B writes buffer
+    // B only after the next barrier, which every phase-G reader has passed.
+  }
+}
+
+// ---------------------------------------------------------------------------
+// dim = 3 geometric factors: qdata[q][e] = det(dx/dX) * w_q.
+// Same thread roles; per coordinate component c the z pass makes B- and
+// G-contracted columns, the y pass the three mixed products, the x pass the
+// three derivatives d x_c / d X_d, kept in registers until the determinant.
+// ---------------------------------------------------------------------------
+template <int P, int Q>
+struct Build3D {
+  static constexpr int E = 8;
+  static constexpr int NT = E * Q * Q;
+  static constexpr int PS1 = plane_stride(P * Q * E, E);
+  static constexpr int PS2 = plane_stride(Q * Q * E, E);
+  static constexpr int S1 = P * PS1;  // one array [py][qz*P+px][e]
+  static constexpr int S2 = P * PS2;  // one array [px][qz*Q+qy][e]
+  static constexpr int SMEM = (2 * S1 + 3 * S2) * 8;
+};
+
+template <int P, int Q>
+__global__ void __launch_bounds__(Build3D<P, Q>::NT, 1) mass3d_build_kernel(
+    const __grid_constant__ Mat1D<P, Q> m, const int* __restrict__ offsets, const double* __restrict__ x,
+    int64_t comp_stride, double* __restrict__ qdata, int num_elem) {
+  using L = Build3D<P, Q>;
+  constexpr int E = L::E;
+  extern __shared__ double smem[];
+  double* s1b = smem;
+  double* s1g = smem + L::S1;
+  double* sbb = smem + 2 * L::S1;
+  double* sgb = sbb + L::S2;
+  double* sbg = sgb + L::S2;
+  const int t = threadIdx.x, e = t % E, col = t / E;
+  const int64_t eg = int64_t(blockIdx.x) * E + e;
+  const bool valid = eg < num_elem;
+  const bool nodal = col < P * P, mixed = col < P * Q;
+  double J[3][3][Q];  // J[d][c][qx] = d x_c / d X_d at (qx, qy, qz)
+
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    if (nodal) {
+      double xz[P];
+      const int* orow = offsets + (valid ? eg : 0) * int64_t(P * P * P) + col;
+#pragma unroll
+      for (int pz = 0; pz < P; ++pz) xz[pz] = __ldg(x + __ldg(orow + pz * P * P) + c * comp_stride);
+      const int px = col % P, py = col / P;
+#pragma unroll
+      for (int qz = 0; qz < Q; ++qz) {
+        double sb = 0.0, sg = 0.0;
+#pragma unroll
+        for (int pz = 0; pz < P; ++pz) {
+          sb += m.B[qz * P + pz] * xz[pz];
+          sg += m.G[qz * P + pz] * xz[pz];
+        }
+        s1b[py * L::PS1 + (qz * P + px) * E + e] = sb;
+        s1g[py * L::PS1 + (qz * P + px) * E + e] = sg;
+      }
+    }
+    __syncthreads();
+    if (mixed) {
+      double yb[P], yg[P];
+#pragma unroll
+      for (int py = 0; py < P; ++py) {
+        yb[py] = s1b[py * L::PS1 + col * E + e];
+        yg[py] = s1g[py * L::PS1 + col * E + e];
+      }
+      const int px = col % P, qz = col / P;
+#pragma unroll
+      for (int qy = 0; qy < Q; ++qy) {
+        double bb = 0.0, gb = 0.0, bg = 0.0;
+#pragma unroll
+        for (int py = 0; py < P; ++py) {
+          bb += m.B[qy * P + py] * yb[py];
+          gb += m.G[qy * P + py] * yb[py];
+          bg += m.B[qy * P + py] * yg[py];
+        }
+        const int idx = px * L::PS2 + (qz * Q + qy) * E + e;
+        sbb[idx] = bb;
+        sgb[idx] = gb;
+        sbg[idx] = bg;
+      }
+    }
+    __syncthreads();
+    {
+      double wbb[P], wgb[P], wbg[P];
+#pragma unroll
+      for (int px = 0; px < P; ++px) {
+        const int idx = px * L::PS2 + col * E + e;
+        wbb[px] = sbb[idx];
+        wgb[px] = sgb[idx];
+        wbg[px] = sbg[idx];
+      }
+#pragma unroll
+      for (int qx = 0; qx < Q; ++qx) {
+        double d0 = 0.0, d1 = 0.0, d2 = 0.0;
+#pragma unroll
+        for (int px = 0; px < P; ++px) {
+          d0 += m.G[qx * P + px] * wbb[px];
+          d1 += m.B[qx * P + px] * wgb[px];
+          d2 += m.B[qx * P + px] * wbg[px];
+        }
+        J[0][c][qx] = d0;
+        J[1][c][qx] = d1;
+        J[2][c][qx] = d2;
+      }
+    }
+    __syncthreads();
+  }
+  if (!valid) return;
+  const int qy = col % Q, qz = col / Q;
+#pragma unroll
+  for (int qx = 0; qx < Q; ++qx) {
+    // include/qfunctions/mass.hpp:27-31, the same cofactor expansion
+    const double det = J[0][0][qx] * (J[1][1][qx] * J[2][2][qx] - J[1][2][qx] * J[2][1][qx]) -
+                       J[0][1][qx] * (J[1][0][qx] * J[2][2][qx] - J[1][2][qx] * J[2][0][qx]) +
+                       J[0][2][qx] * (J[1][0][qx] * J[2][1][qx] - J[1][1][qx] * J[2][0][qx]);
+    const double w = m.W[qz] * (m.W[qy] * m.W[qx]);  // src/tensor-contract.cpp:169-192 product order
+    qdata[(int64_t((qz * Q + qy) * Q + qx)) * num_elem + eg] = det * w;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// dim = 2 fused apply.  E = 32 elements, 32*Q threads; a thread owns a column
+// along y.  phase A (px): gather, contract y -> S1[px][qy][e];
+// phase C (qy): contract x, times qdata, contract x^T -> S3[qy][px][e];
+// phase G (px): contract y^T, scatter.
+// ---------------------------------------------------------------------------
+template <int P, int Q>
+struct Mass2D {
+  static constexpr int E = 32;
+  static constexpr int NT = E * Q;
+  static constexpr int S1 = P * Q * E, S3 = Q * P * E;
+  static constexpr int SMEM = (S1 + S3) * 8;
+  static constexpr int ES = P * P, NQ = Q * Q;
+};
+
+template <int P, int Q>
+__global__ void __launch_bounds__(Mass2D<P, Q>::NT) mass2d_apply_kernel(
+    const __grid_constant__ Mat1D<P, Q> m, const int* __restrict__ offs, const double* __restrict__ qd,
+    const double* __restrict__ u, double* __restrict__ v, double* __restrict__ ev, int num_elem, int num_comp_run,
+    int64_t comp_stride) {
+  using L = Mass2D<P, Q>;
+  constexpr int E = L::E;
+  extern __shared__ double smem[];
+  double* s1 = smem;
+  double* s3 = smem + L::S1;
+  const int t = threadIdx.x, e = t % E, col = t / E;
+  const int64_t tile = blockIdx.x;
+  const int64_t eg = tile * E + e;
+  const bool valid = eg < num_elem;
+  const bool nodal = col < P;
+  double qv[Q];
+  {
+    const double* qt = qd + tile * (int64_t(L::NQ) * E) + col * E + e;
+#pragma unroll
+    for (int qx = 0; qx < Q; ++qx) qv[qx] = __ldg(qt + qx * (Q * E));
+  }
+  int off[P];
+  if (nodal) {
+    const int* ot = offs + tile * (int64_t(L::ES) * E) + col * E + e;
+#pragma unroll
+    for (int py = 0; py < P; ++py) off[py] = __ldg(ot + py * (P * E));
+  }
+  for (int k = 0; k < num_comp_run; ++k) {
+    const int64_t ks = k * comp_stride;
+    if (nodal) {
+      double x[P];
+#pragma unroll
+      for (int py = 0; py < P; ++py) x[py] = __ldg(u + off[py] + ks);
+#pragma unroll
+      for (int qy = 0; qy < Q; ++qy) {
+        double s = 0.0;
+#pragma unroll
+        for (int py = 0; py < P; ++py) s += m.B[qy * P + py] * x[py];
+        s1[(col * Q + qy) * E + e] = s;
+      }
+    }
+    __syncthreads();
+    {
+      double w[P];
+#pragma unroll
+      for (int px = 0; px < P; ++px) w[px] = s1[(px * Q + col) * E + e];
+      double r[Q];
+#pragma unroll
+      for (int qx = 0; qx < Q; ++qx) {
+        double s = 0.0;
+#pragma unroll
+        for (int px = 0; px < P; ++px) s += m.B[qx * P + px] * w[px];
+        r[qx] = qv[qx] * s;
+      }
+#pragma unroll
+      for (int px = 0; px < P; ++px) {
+        double s = 0.0;
+#pragma unroll
+        for (int qx = 0; qx < Q; ++qx) s += m.B[qx * P + px] * r[qx];
+        s3[(col * P + px) * E + e] = s;
+      }
+    }
+    __syncthreads();
+    if (nodal) {
+      double z[Q];
+#pragma unroll
+      for (int qy = 0; qy < Q; ++qy) z[qy] = s3[(qy * P + col) * E + e];
+#pragma unroll
+      for (int py = 0; py < P; ++py) {
+        double s = 0.0;
+#pragma unroll
+        for (int qy = 0; qy < Q; ++qy) s += m.B[qy * P + py] * z[qy];
+        if (valid) {
+          if (ev)
+            ev[(int64_t(k) * L::ES + py * P + col) * num_elem + eg] = s;
+          else
+            atomicAdd(v + off[py] + ks, s);
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <int P, int Q>
+__global__ void __launch_bounds__(32 * Q) mass2d_build_kernel(const __grid_constant__ Mat1D<P, Q> m,
+                                                             const int* __restrict__ offsets,
+                                                             const double* __restrict__ x, int64_t comp_stride,
+                                                             double* __restrict__ qdata, int num_elem) {
+  constexpr int E = 32;
+  __shared__ double s1b[P * Q * E], s1g[P * Q * E];
+  const int t = threadIdx.x, e = t % E, col = t / E;
+  const int64_t eg = int64_t(blockIdx.x) * E + e;
+  const bool valid = eg < num_elem;
+  double J[2][2][Q];
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+    if (col < P) {
+      double xy[P];
+      const int* orow = offsets + (valid ? eg : 0) * int64_t(P * P) + col;
+#pragma unroll
+      for (int py = 0; py < P; ++py) xy[py] = __ldg(x + __ldg(orow + py * P) + c * comp_stride);
+#pragma unroll
+      for (int qy = 0; qy < Q; ++qy) {
+        double sb = 0.0, sg = 0.0;
+#pragma unroll
+        for (int py = 0; py < P; ++py) {
+          sb += m.B[qy * P + py] * xy[py];
+          sg += m.G[qy * P + py] * xy[py];
+        }
+        s1b[(col * Q + qy) * E + e] = sb;
+        s1g[(col * Q + qy) * E + e] = sg;
+      }
+    }
+    __syncthreads();
+    {
+      double wb[P], wg[P];
+#pragma unroll
+      for (int px = 0; px < P; ++px) {
+        wb[px] = s1b[(px * Q + col) * E + e];
+        wg[px] = s1g[(px * Q + col) * E + e];
+      }
+#pragma unroll
+      for (int qx = 0; qx < Q; ++qx) {
+        double d0 = 0.0, d1 = 0.0;
+#pragma unroll
+        for (int px = 0; px < P; ++px) {
+          d0 += m.G[qx * P + px] * wb[px];
+          d1 += m.B[qx * P + px] * wg[px];
+        }
+        J[0][c][qx] = d0;
+        J[1][c][qx] = d1;
+      }
+    }
+    __syncthreads();
+  }
+  if (!valid) return;
+  const int qy = col;
+#pragma unroll
+  for (int qx = 0; qx < Q; ++qx) {
+    const double det = J[0][0][qx] * J[1][1][qx] - J[0][1][qx] * J[1][0][qx];
+    const double w = m.W[qy] * m.W[qx];
+    qdata[int64_t(qy * Q + qx) * num_elem + eg] = det * w;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// dim = 1: one thread per element, everything in registers.
+// ---------------------------------------------------------------------------
+template <int P, int Q>
+__global__ void __launch_bounds__(128) mass1d_apply_kernel(const __grid_constant__ Mat1D<P, Q> m,
+                                                          const int* __restrict__ offs, const double* __restrict__ qd,
+                                                          const double* __restrict__ u, double* __restrict__ v,
+                                                          double* __restrict__ ev, int num_elem, int num_comp_run,
+                                                          int64_t comp_stride) {
+  constexpr int E = 128;
+  const int e = threadIdx.x;
+  const int64_t tile = blockIdx.x, eg = tile * E + e;
+  if (eg >= num_elem) return;
+  int off[P];
+  double qv[Q];
+#pragma unroll
+  for (int px = 0; px < P; ++px) off[px] = __ldg(offs + (tile * P + px) * E + e);
+#pragma unroll
+  for (int qx = 0; qx < Q; ++qx) qv[qx] = __ldg(qd + (tile * Q + qx) * E + e);
+  for (int k = 0; k < num_comp_run; ++k) {
+    const int64_t ks = k * comp_stride;
+    double x[P], r[Q];
+#pragma unroll
+    for (int px = 0; px < P; ++px) x[px] = __ldg(u + off[px] + ks);
+#pragma unroll
+    for (int qx = 0; qx < Q; ++qx) {
+      double s = 0.0;
+#pragma unroll
+      for (int px = 0; px < P; ++px) s += m.B[qx * P + px] * x[px];
+      r[qx] = qv[qx] * s;
+    }
+#pragma unroll
+    for (int px = 0; px < P; ++px) {
+      double s = 0.0;
+#pragma unroll
+      for (int qx = 0; qx < Q; ++qx) s += m.B[qx * P + px] * r[qx];
+      if (ev)
+        ev[(int64_t(k) * P + px) * num_elem + eg] = s;
+      else
+        atomicAdd(v + off[px] + ks, s);
+    }
+  }
+}
+
+template <int P, int Q>
+__global__ void __launch_bounds__(128) mass1d_build_kernel(const __grid_constant__ Mat1D<P, Q> m,
+                                                          const int* __restrict__ offsets,
+                                                          const double* __restrict__ x, int64_t comp_stride,
+                                                          double* __restrict__ qdata, int num_elem) {
+  const int64_t eg = int64_t(blockIdx.x) * 128 + threadIdx.x;
+  if (eg >= num_elem) return;
+  double xe[P];
+#pragma unroll
+  for (int px = 0; px < P; ++px) xe[px] = __ldg(x + __ldg(offsets + eg * P + px));
+#pragma unroll
+  for (int qx = 0; qx < Q; ++qx) {
+    double d = 0.0;
+#pragma unroll
+    for (int px = 0; px < P; ++px) d += m.G[qx * P + px] * xe[px];
+    qdata[int64_t(qx) * num_elem + eg] = d * m.W[qx];
+  }
+}
+
+}  // namespace fem_b200

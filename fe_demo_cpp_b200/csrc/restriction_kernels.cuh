@@ -1,0 +1,139 @@
+// Standalone element-restriction and basis kernels (sm_100a).
+//
+// Restriction layouts are the reference's (src/elem-restriction.cpp:34-83):
+//   E[(k*elem_size + i)*num_elem + e]  <->  L[offsets[e*elem_size + i] + k*comp_stride]
+// The offsets are row-major [e][i] (i fastest) while the E-vector has e
+// fastest, so a direct thread mapping coalesces only one side (the
+// reference's kernels, src/cuda/cuda-elem-restriction.cu:37-67, coalesce the
+// offsets).  Here a 32-element x 32-node tile of offsets is staged through
+// shared memory, so both the offsets reads and the E-vector accesses are
+// contiguous across a warp.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace fem_b200 {
+
+constexpr int kTile = 32;
+
+// mode 0: gather  E = L[offsets]        (out = E, overwritten)
+// mode 1: scatter L[offsets] += E       (atomic)
+// mode 2: count   L[offsets] += 1.0     (multiplicity numerator, E unused)
+template <int MODE>
+__global__ void __launch_bounds__(kTile * 8) offset_tile_kernel(const int* __restrict__ offsets, int num_elem,
+                                                               int elem_size, int num_comp, int64_t comp_stride,
+                                                               const double* __restrict__ in, double* __restrict__ out) {
+  __shared__ int so[kTile][kTile + 1];
+  const int i0 = blockIdx.x * kTile;
+  const int64_t e0 = int64_t(blockIdx.y) * kTile;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  // read: lanes along the node index (contiguous offsets)
+  for (int r = ty; r < kTile; r += 8) {
+    const int64_t e = e0 + r;
+    const int i = i0 + tx;
+    so[r][tx] = (e < num_elem && i < elem_size) ? offsets[e * elem_size + i] : -1;
+  }
+  __syncthreads();
+  // write: lanes along the element index (contiguous E-vector)
+  const int64_t e = e0 + tx;
+  if (e >= num_elem) return;
+  for (int c = ty; c < kTile; c += 8) {
+    const int i = i0 + c;
+    if (i >= elem_size) break;
+    const int64_t off = so[tx][c];
+    for (int k = 0; k < num_comp; ++k) {
+      const int64_t ev = (int64_t(k) * elem_size + i) * num_elem + e;
+      const int64_t lv = off + k * comp_stride;
+      if (MODE == 0)
+        out[ev] = __ldg(in + lv);
+      else if (MODE == 1)
+        atomicAdd(out + lv, __ldg(in + ev));
+      else
+        atomicAdd(out + lv, 1.0);
+    }
+  }
+}
+
+// Deterministic scatter-add through the transpose map: one thread per used
+// L-node, summing its E-entries in increasing t = i + e*elem_size (the order
+// of the reference's CPU scatter, src/elem-restriction.cpp:73-82, and of its
+// CUDA deterministic kernel, src/cuda/cuda-elem-restriction.cu:75-95), then
+// one add into v.
+__global__ void csr_scatter_kernel(int num_nodes, int num_elem, int elem_size, int num_comp, int64_t comp_stride,
+                                   const int* __restrict__ l_vec_indices, const int* __restrict__ t_offsets,
+                                   const int* __restrict__ t_indices, const double* __restrict__ ev,
+                                   double* __restrict__ v) {
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < num_nodes; n += gridDim.x * blockDim.x) {
+    const int64_t l = l_vec_indices[n];
+    const int t0 = t_offsets[n], t1 = t_offsets[n + 1];
+    for (int k = 0; k < num_comp; ++k) {
+      double sum = 0.0;
+      for (int t = t0; t < t1; ++t) {
+        const int ti = t_indices[t];
+        const int e = ti / elem_size, i = ti - e * elem_size;
+        sum += ev[(int64_t(k) * elem_size + i) * num_elem + e];
+      }
+      v[l + k * comp_stride] += sum;
+    }
+  }
+}
+
+// Strided gather (mode 0) / scatter-add (mode 1), one thread per E entry in
+// E order; with backend strides both sides are the same contiguous array.
+template <int MODE>
+__global__ void strided_kernel(int num_elem, int elem_size, int num_comp, int64_t s0, int64_t s1, int64_t s2,
+                               const double* __restrict__ in, double* __restrict__ out) {
+  const int64_t n = int64_t(num_elem) * elem_size * num_comp;
+  for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < n; t += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t e = t % num_elem, rest = t / num_elem;
+    const int64_t i = rest % elem_size, k = rest / elem_size;
+    const int64_t l = i * s0 + k * s1 + e * s2;
+    if (MODE == 0)
+      out[t] = in[l];
+    else
+      out[l] += in[t];
+  }
+}
+
+// One pass of the batched 1D contraction (the reference's single primitive,
+// src/tensor-contract.cpp:35-59):
+//   v[(a*J + j)*C + c] (+)= sum_b t(j,b) u[(a*B + b)*C + c]
+// one thread per output, c fastest (c runs over the already-contracted axes
+// and the elements, so warps read and write contiguous runs).
+// t(j,b) = t[j*B + b] (NoTranspose) or t[b*J + j] (Transpose).
+__global__ void contract_kernel(int64_t A, int B, int64_t C, int J, const double* __restrict__ t, int transpose,
+                                int add, const double* __restrict__ u, double* __restrict__ v) {
+  const int64_t n = A * J * C;
+  const int64_t s0 = transpose ? 1 : B, s1 = transpose ? J : 1;
+  for (int64_t o = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; o < n; o += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t c = o % C, rest = o / C;
+    const int64_t j = rest % J, a = rest / J;
+    const double* up = u + a * B * C + c;
+    double s = 0.0;
+    for (int b = 0; b < B; ++b) s += __ldg(t + j * s0 + b * s1) * __ldg(up + b * C);
+    if (add)
+      v[o] += s;
+    else
+      v[o] = s;
+  }
+}
+
+// Tensor-product quadrature weights v[q*num_elem + e] = prod_d w[q_d], formed
+// in the reference's order w_z*(w_y*w_x) (src/tensor-contract.cpp:169-192).
+__global__ void weight_kernel(int dim, int Q, const double* __restrict__ w1, int num_elem, double* __restrict__ v) {
+  int nq = 1;
+  for (int d = 0; d < dim; ++d) nq *= Q;
+  const int64_t n = int64_t(nq) * num_elem;
+  for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < n; t += int64_t(gridDim.x) * blockDim.x) {
+    int q = int(t / num_elem);
+    double w = 1.0;
+    for (int d = 0; d < dim; ++d) {
+      w = w1[q % Q] * (d == 0 ? 1.0 : w);
+      q /= Q;
+    }
+    v[t] = w;
+  }
+}
+
+}  // namespace fem_b200

@@ -1,0 +1,207 @@
+/*
+ * fem_b200.h -- C ABI of libfem_b200, the B200 (sm_100a) matrix-free mass
+ * operator behind the fe-demo-cpp API.
+ *
+ * Plain C: pointers and sizes only, no C++ or torch types.  Every function
+ * returns a status (FEM_B200_SUCCESS = 0); on failure fem_b200_last_error()
+ * returns the message of the calling thread's last failure.  The C++ drop-in
+ * (the headers under include/fem/) turns FEM_B200_ERROR_ARGUMENT into
+ * std::invalid_argument and every other failure into std::runtime_error,
+ * the exception split of the reference.
+ *
+ * Memory: "device" arrays are CUDA global memory of the current device,
+ * "host" arrays are ordinary (preferably pinned) host memory.  A `stream`
+ * argument is a cudaStream_t (NULL = the legacy default stream); device work
+ * is asynchronous on it, like the reference's CUDA restriction
+ * (include/cuda/cuda-elem-restriction.hpp:106-111).
+ *
+ * Layouts are the reference's:
+ *   L-vector   node n, component k at offsets[...] + k*comp_stride
+ *   E-vector   E[(k*elem_size + i)*num_elem + e]      (include/elem-restriction.hpp:49-51)
+ *   Q-vector   [comp][q][e]; Grad output [d][comp][q][e]  (include/tensor-contract.hpp:30-33)
+ *   qdata      backend-strided [q][e]                  (include/elem-restriction.hpp:53-56)
+ * Local nodes and quadrature points are lexicographic with x fastest.
+ */
+#ifndef FEM_B200_H
+#define FEM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+#define FEM_B200_SUCCESS 0
+#define FEM_B200_ERROR_ARGUMENT 1    /* bad size / index / mode (std::invalid_argument) */
+#define FEM_B200_ERROR_CUDA 2        /* a CUDA call or a device status failed */
+#define FEM_B200_ERROR_UNSUPPORTED 3 /* valid, but not on the device path (no CPU fallback) */
+
+/* ---- enums, numbered as the reference's ---------------------------------- */
+/* ContractMode, include/transpose-mode.hpp:13 */
+#define FEM_B200_NOTRANSPOSE 0
+#define FEM_B200_TRANSPOSE 1
+/* EvalMode, include/eval-mode.hpp:11 */
+#define FEM_B200_EVAL_NONE 0
+#define FEM_B200_EVAL_INTERP 1
+#define FEM_B200_EVAL_GRAD 2
+#define FEM_B200_EVAL_WEIGHT 3
+/* QuadMode, include/basis.hpp:21 */
+#define FEM_B200_QUAD_GAUSS 0
+#define FEM_B200_QUAD_GAUSS_LOBATTO 1
+/* fem::cuda::ScatterMode, include/cuda/cuda-elem-restriction.hpp:10-21 */
+#define FEM_B200_SCATTER_ATOMIC 0
+#define FEM_B200_SCATTER_DETERMINISTIC 1
+/* Device QFunctions (the host side matches fem::qfunctions by pointer) */
+#define FEM_B200_QF_APPLY_MASS 0        /* include/qfunctions/mass.hpp:45-51: component 0 only */
+#define FEM_B200_QF_APPLY_MASS_VECTOR 1 /* every component: v_k = qdata * u_k (no reference counterpart) */
+
+typedef struct fem_b200_restriction_s *fem_b200_restriction;
+typedef struct fem_b200_basis_s *fem_b200_basis;
+typedef struct fem_b200_mass_s *fem_b200_mass;
+
+/* Message of this thread's last failure ("" if none). */
+const char *fem_b200_last_error(void);
+/* Library version, major*10000 + minor*100 + patch. */
+int fem_b200_version(void);
+/* Number of visible CUDA devices (0 without a usable GPU; never fails). */
+int fem_b200_device_count(void);
+
+/* ========================================================================= */
+/* Host set-up (no GPU needed)                                                */
+/* ========================================================================= */
+
+/* Gauss-Legendre points/weights on [-1,1], Q >= 1.
+ * Replaces fem::gauss_legendre_quadrature, src/basis.cpp:16-68. */
+int fem_b200_gauss_legendre(int Q, double *x, double *w);
+
+/* Gauss-Lobatto points on [-1,1] (ascending), Q >= 2; w may be NULL.
+ * Replaces fem::gauss_lobatto_points, src/basis.cpp:81-144. */
+int fem_b200_gauss_lobatto(int Q, double *x, double *w);
+
+/* Lagrange interpolation / derivative matrices [M][P] of the basis on
+ * `nodes` (P) evaluated at `pts` (M).
+ * Replaces fem::lagrange_basis_matrix, src/basis.cpp:156-186. */
+int fem_b200_lagrange_basis_matrix(int P, const double *nodes, int M, const double *pts, double *interp,
+                                   double *grad);
+
+/* 1D data of the tensor-product H1 Lagrange basis (GLL nodes): q_ref[Q],
+ * q_weight[Q], interp[Q*P], grad[Q*P]; dim 1..3, num_comp 1..3, P >= 2, Q >= 1.
+ * Replaces fem::TensorBasis::create_tensor_H1_lagrange, src/basis.cpp:202-228. */
+int fem_b200_tensor_h1_lagrange(int dim, int num_comp, int P, int Q, int quad_mode, double *q_ref, double *q_weight,
+                                double *interp, double *grad);
+
+/* Validation of an offset restriction (n_offsets = entries given).
+ * Replaces the checks of fem::elem_restriction_create, src/elem-restriction.cpp:102-138. */
+int fem_b200_restriction_check_offset(int num_elem, int elem_size, int num_comp, int comp_stride, int l_size,
+                                      const int *offsets, int64_t n_offsets);
+
+/* Validation of a strided restriction; strides NULL = backend strides
+ * {num_elem, elem_size*num_elem, 1}.
+ * Replaces the checks of fem::elem_restriction_create_strided, src/elem-restriction.cpp:155-204. */
+int fem_b200_restriction_check_strided(int num_elem, int elem_size, int num_comp, int l_size, const int *strides);
+
+/* Transpose map (CSR inverse of the offsets) on the host.  Sizes: l_vec_indices
+ * and t_offsets at least l_size and l_size+1, t_indices num_elem*elem_size;
+ * *num_nodes receives the number of used L-nodes.
+ * Replaces fem::cuda::build_transpose_map, src/cuda/cuda-elem-restriction.cu:149-177. */
+int fem_b200_transpose_map(int num_elem, int elem_size, int l_size, const int *offsets, int *l_vec_indices,
+                           int *t_offsets, int *t_indices, int *num_nodes);
+
+/* ========================================================================= */
+/* Element restriction on the device                                          */
+/* ========================================================================= */
+
+/* Offset restriction from host offsets [num_elem][elem_size]; validated as
+ * above, uploaded once.  SCATTER_DETERMINISTIC also builds the transpose map.
+ * Replaces fem::cuda::elem_restriction_create, src/cuda/cuda-elem-restriction.cu:188-215. */
+int fem_b200_restriction_create_offset(int num_elem, int elem_size, int num_comp, int comp_stride, int l_size,
+                                       const int *offsets, int scatter_mode, fem_b200_restriction *out);
+
+/* Strided restriction; strides NULL = backend strides.
+ * Replaces fem::cuda::elem_restriction_create on a strided restriction. */
+int fem_b200_restriction_create_strided(int num_elem, int elem_size, int num_comp, int l_size, const int *strides,
+                                        fem_b200_restriction *out);
+
+int fem_b200_restriction_destroy(fem_b200_restriction r);
+
+/* Sizes of a restriction (any pointer may be NULL). */
+int fem_b200_restriction_sizes(fem_b200_restriction r, int *num_elem, int *elem_size, int *num_comp, int *l_size,
+                               int64_t *e_size);
+
+/* Device transpose map (deterministic offset restrictions): copies it into
+ * host arrays sized as for fem_b200_transpose_map. */
+int fem_b200_restriction_transpose_map(fem_b200_restriction r, int *l_vec_indices, int *t_offsets, int *t_indices,
+                                       int *num_nodes);
+
+/* NoTranspose: out (device, e_size) = gather of in (device, l_size).
+ * Transpose:   out (device, l_size) += scatter of in (device, e_size).
+ * Replaces fem::cuda::elem_restriction_apply, src/cuda/cuda-elem-restriction.cu:230-273,
+ * and fem::elem_restriction_apply, src/elem-restriction.cpp:34-83. */
+int fem_b200_restriction_apply(fem_b200_restriction r, int t_mode, const double *in, int64_t n_in, double *out,
+                               int64_t n_out, void *stream);
+
+/* mult (device, l_size) = E^T(E 1), overwritten.
+ * Replaces fem::elem_restriction_get_multiplicity, src/elem-restriction.cpp:215-227. */
+int fem_b200_restriction_multiplicity(fem_b200_restriction r, double *mult, int64_t n, void *stream);
+
+/* ========================================================================= */
+/* Tensor basis on the device                                                 */
+/* ========================================================================= */
+
+int fem_b200_basis_create(int dim, int num_comp, int P, int Q, int quad_mode, fem_b200_basis *out);
+int fem_b200_basis_destroy(fem_b200_basis b);
+
+/* v (device) = basis action on u (device) for num_elem elements.  Interp and
+ * Grad in both directions, Weight NoTranspose (u ignored).  v is overwritten
+ * in every mode (the reference's Grad Transpose adds into a stale v,
+ * src/tensor-contract.cpp:115-145; on a zeroed v both agree).
+ * Replaces fem::tensor_basis_apply, src/tensor-contract.cpp:207-222. */
+int fem_b200_basis_apply(fem_b200_basis b, int num_elem, int t_mode, int eval_mode, const double *u, int64_t n_u,
+                         double *v, int64_t n_v, void *stream);
+
+/* ========================================================================= */
+/* Mass operator                                                              */
+/* ========================================================================= */
+
+/* qdata (device, Q^dim*num_elem, [q][e]) = det(dx/dX) * w from the coordinate
+ * L-vector x (device) of restriction rx (num_comp = dim) and basis bx
+ * (num_comp = dim): the build operator of the reference, fused.
+ * Replaces operator_apply on the build_mass operator, src/operator.cpp:148-182
+ * with include/qfunctions/mass.hpp:17-40. */
+int fem_b200_mass_build(fem_b200_restriction rx, fem_b200_basis bx, const double *x, int64_t n_x, double *qdata,
+                        int64_t n_qdata, void *stream);
+
+/* Mass operator v = E^T B^T D B E u on restriction ru / basis bu with the
+ * backend-strided qdata (device, [q][e]); the plan keeps its own copy of
+ * qdata (laid out for the kernel), as the reference Operator copies passive
+ * vectors (include/operator.hpp:33-47).  qf: FEM_B200_QF_APPLY_MASS or
+ * FEM_B200_QF_APPLY_MASS_VECTOR.  The scatter mode is ru's.
+ * Replaces operator_create + operator_set_field on the mass QFunction,
+ * src/operator.cpp:21-117. */
+int fem_b200_mass_create(fem_b200_restriction ru, fem_b200_basis bu, const double *qdata, int64_t n_qdata, int qf,
+                         fem_b200_mass *out);
+int fem_b200_mass_destroy(fem_b200_mass op);
+
+/* v (device, l_size) = M u (device, l_size): zeroed, then summed into.
+ * Replaces fem::operator_apply, src/operator.cpp:148-182. */
+int fem_b200_mass_apply(fem_b200_mass op, const double *u, int64_t n_u, double *v, int64_t n_v, void *stream);
+
+/* v += M u (device arrays), no zeroing. */
+int fem_b200_mass_apply_add(fem_b200_mass op, const double *u, int64_t n_u, double *v, int64_t n_v, void *stream);
+
+/* Host-memory form of fem_b200_mass_apply: copies u in, applies, copies v out
+ * on `stream` through plan-owned device buffers, then synchronizes the stream.
+ * The call a host std::vector user makes (operator_apply(op, in, out)). */
+int fem_b200_mass_apply_host(fem_b200_mass op, const double *u_host, int64_t n_u, double *v_host, int64_t n_v,
+                             void *stream);
+
+/* Number of kernel launches one fem_b200_mass_apply makes, and the plan's
+ * element-tile size and device footprint in bytes (any pointer may be NULL). */
+int fem_b200_mass_info(fem_b200_mass op, int *launches_per_apply, int *tile_elems, int64_t *device_bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FEM_B200_H */
