@@ -69,10 +69,14 @@ def _mesh(dim, shape, P, seed):
 
 @pytest.mark.parametrize("dim,shape,P,Q", SHAPES)
 def test_build_qdata_matches_oracle(fem, cuda, orc, dim, shape, P, Q):
+    """J = sum_p G_qp x_p is formed from O(1) absolute coordinates whose
+    differences are O(h): the reference and the device both lose about
+    log10(1/h) digits to that cancellation (with different rounding), so
+    qdata is compared at TOL / h, h = 1 / (elements per side)."""
     m = _mesh(dim, shape, P, seed=3)
     qd = host(build_qdata(fem, cuda, m, Q))
     want = orc.mass_build(dim, m.num_elem, P, Q, m.num_nodes, m.offsets, m.coords)
-    close(qd, want)
+    close(qd, want, TOL * max(shape))
 
 
 @pytest.mark.parametrize("scatter", [0, 1], ids=["atomic", "deterministic"])
@@ -123,7 +127,7 @@ def test_golden_config1_matches_reference(fem, cuda, golden):
     m = box_mesh((8, 8, 8), 4, seed=1)
     assert m.digest() == str(golden[name + "_mesh_sha"])
     qd = build_qdata(fem, cuda, m, 5)
-    close(host(qd).reshape(-1, m.num_elem).sum(0), golden[name + "_qdata_elemsum"])
+    close(host(qd).reshape(-1, m.num_elem).sum(0), golden[name + "_qdata_elemsum"], TOL * 8)
     for scatter in (0, 1):
         op = fem.MassOperator(fem.Restriction(m.num_elem, 64, 1, m.num_nodes, m.num_nodes, m.offsets, scatter),
                               fem.Basis(3, 1, 4, 5), qd)
