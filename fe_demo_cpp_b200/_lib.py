@@ -38,6 +38,7 @@ SIGNATURES = {
     "fem_b200_basis_create": ([_i, _i, _i, _i, _i, _p], _i),
     "fem_b200_basis_destroy": ([_p], _i),
     "fem_b200_basis_apply": ([_p, _i, _i, _i, _p, _i64, _p, _i64, _p], _i),
+    "fem_b200_basis_apply_static": ([_p, _i, _i, _i, _p, _i64, _p, _i64, _p], _i),
     "fem_b200_mass_build": ([_p, _p, _p, _i64, _p, _i64, _p], _i),
     "fem_b200_mass_create": ([_p, _p, _p, _i64, _i, _p], _i),
     "fem_b200_mass_destroy": ([_p], _i),

@@ -276,6 +276,33 @@ struct fem_b200_mass_s {
 };
 
 // ===========================================================================
+// Scratch for fem_b200_basis_apply_static: the ping-pong pass buffers of the
+// basis contractions, in a fixed device array instead of cudaMalloc'd memory.
+// Every GPU that loads this library holds it (16 MiB) until the process exits.
+// ===========================================================================
+static constexpr int64_t kStaticScratchDoubles = int64_t(1) << 21;  // 2,097,152 doubles = 16 MiB
+static __device__ __align__(256) double g_basis_static_scratch[kStaticScratchDoubles];
+
+namespace {
+std::mutex g_static_scratch_mu;
+double* g_static_scratch_ptr[64] = {};
+
+// Device address of g_basis_static_scratch on the current device `dev`.  In
+// host code the symbol itself is only a host-side stand-in, never a device
+// address, so the address is looked up once per device and cached.
+double* static_scratch_on(int dev) {
+  require(dev >= 0 && dev < 64, "basis apply (static scratch): device index out of range");
+  std::lock_guard<std::mutex> lock(g_static_scratch_mu);
+  if (!g_static_scratch_ptr[dev]) {
+    void* p = nullptr;
+    FEM_CUDA_CHECK(cudaGetSymbolAddress(&p, g_basis_static_scratch));
+    g_static_scratch_ptr[dev] = static_cast<double*>(p);
+  }
+  return g_static_scratch_ptr[dev];
+}
+}  // namespace
+
+// ===========================================================================
 // extern "C" entry points
 // ===========================================================================
 extern "C" {
@@ -555,6 +582,64 @@ int fem_b200_basis_apply(fem_b200_basis b, int num_elem, int t_mode, int eval_mo
     std::lock_guard<std::mutex> lock(bd.scratch_mu);
     if (h.dim > 1 && bd.scratch.size() < size_t(2 * big)) bd.scratch.alloc(size_t(2 * big));
     double* tmp[2] = {bd.scratch.get(), bd.scratch.get() + big};
+    const int naxes = grad ? h.dim : 1;
+    for (int ax = 0; ax < naxes; ++ax) {
+      int64_t pre = h.num_comp * ipow(P, h.dim - 1), post = num_elem;
+      for (int dd = 0; dd < h.dim; ++dd) {
+        const double* mat = (grad && dd == ax) ? bd.grad.get() : bd.interp.get();
+        const double* src = dd == 0 ? (tr && grad ? u + ax * qn : u) : tmp[dd % 2];
+        const bool last = dd == h.dim - 1;
+        double* dst = last ? (tr ? v : (grad ? v + ax * qn : v)) : tmp[(dd + 1) % 2];
+        const int add = (last && tr && grad && ax > 0) ? 1 : 0;
+        const int64_t n = pre * Q * post;
+        contract_kernel<<<grid_for(n, 256), 256, 0, s>>>(pre, P, post, Q, mat, tr ? 1 : 0, add, src, dst);
+        FEM_LAUNCH_CHECK();
+        pre /= P;
+        post *= Q;
+      }
+    }
+  });
+}
+
+// Same contractions as fem_b200_basis_apply, with the pass buffers in
+// g_basis_static_scratch: nothing is allocated.  Each pass overwrites the
+// scratch it writes, so nothing has to be cleared between calls.
+int fem_b200_basis_apply_static(fem_b200_basis b, int num_elem, int t_mode, int eval_mode, const double* u,
+                                int64_t n_u, double* v, int64_t n_v, void* stream) {
+  return guarded([&] {
+    require(b && b->d, "tensor_basis_apply: NULL handle");
+    BasisDev& bd = *b->d;
+    const BasisData& h = bd.h;
+    const bool tr = t_mode == FEM_B200_TRANSPOSE;
+    require(t_mode == FEM_B200_NOTRANSPOSE || tr, "tensor_basis_apply: unknown t_mode");
+    require(num_elem > 0, "tensor_basis_apply: num_elem must be positive");
+    const int64_t pn = ipow(h.P, h.dim) * h.num_comp * num_elem;
+    const int64_t qn = ipow(h.Q, h.dim) * h.num_comp * num_elem;
+    DeviceGuard g(bd.device);
+    cudaStream_t s = as_stream(stream);
+    if (eval_mode == FEM_B200_EVAL_WEIGHT) {
+      require(!tr, "EvalMode::Weight is incompatible with ContractMode::Transpose");
+      require(n_v == ipow(h.Q, h.dim) * num_elem && v, "tensor_basis_apply: v has the wrong size");
+      weight_kernel<<<grid_for(n_v, 256), 256, 0, s>>>(h.dim, h.Q, bd.weight.get(), num_elem, v);
+      FEM_LAUNCH_CHECK();
+      return;
+    }
+    require(eval_mode == FEM_B200_EVAL_INTERP || eval_mode == FEM_B200_EVAL_GRAD,
+            "tensor_basis_apply: unknown eval_mode");
+    const bool grad = eval_mode == FEM_B200_EVAL_GRAD;
+    const int64_t in_n = tr ? (grad ? h.dim * qn : qn) : pn;
+    const int64_t out_n = tr ? pn : (grad ? h.dim * qn : qn);
+    require(n_u == in_n && u, "tensor_basis_apply: u has the wrong size");
+    require(n_v == out_n && v, "tensor_basis_apply: v has the wrong size");
+    const int P = tr ? h.Q : h.P, Q = tr ? h.P : h.Q;
+    const int64_t big = h.num_comp * ipow(std::max(h.P, h.Q), h.dim) * num_elem;
+    const int64_t need = h.dim > 1 ? 2 * big : 0;
+    if (need > kStaticScratchDoubles)
+      throw arg_error("tensor_basis_apply (static scratch): this call needs " + std::to_string(need) +
+                      " doubles of scratch (2 * num_comp * max(P,Q)^dim * num_elem) but the static scratch holds " +
+                      std::to_string(kStaticScratchDoubles) + " (16 MiB); split the elements into smaller calls");
+    double* scratch = static_scratch_on(bd.device);
+    double* tmp[2] = {scratch, scratch + big};
     const int naxes = grad ? h.dim : 1;
     for (int ax = 0; ax < naxes; ++ax) {
       int64_t pre = h.num_comp * ipow(P, h.dim - 1), post = num_elem;

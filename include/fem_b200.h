@@ -161,6 +161,26 @@ int fem_b200_basis_destroy(fem_b200_basis b);
 int fem_b200_basis_apply(fem_b200_basis b, int num_elem, int t_mode, int eval_mode, const double *u, int64_t n_u,
                          double *v, int64_t n_v, void *stream);
 
+/* Allocation-free form of fem_b200_basis_apply (no counterpart in the
+ * reference).  fem_b200_basis_apply keeps its pass buffers in device memory
+ * that it allocates with cudaMalloc on its first call and whenever num_elem
+ * grows.  Some callers cannot allow that: code that is being captured into a
+ * CUDA graph (cudaMalloc is not permitted during a global-mode capture), hosts
+ * whose device memory is owned by another allocator or a fixed budget, and
+ * loops that must not stall on the allocator.  This entry point takes the same
+ * arguments and computes the same result, with the pass buffers in a fixed
+ * array compiled into the library: 2,097,152 doubles (16 MiB), which every
+ * GPU that loads the library holds until the process exits.  A call needing
+ * more (2 * num_comp * max(P,Q)^dim * num_elem doubles for dim > 1) fails with
+ * FEM_B200_ERROR_ARGUMENT; split the elements over several calls.  The first
+ * call on a device looks up the array's device address (set-up that may load
+ * the module), so make that first call before any stream capture.  All calls
+ * share the one array: calls that overlap on the GPU (other streams, other
+ * host threads) race and must be serialised by the caller.  Each pass
+ * overwrites the scratch it uses, so nothing needs clearing between calls. */
+int fem_b200_basis_apply_static(fem_b200_basis b, int num_elem, int t_mode, int eval_mode, const double *u,
+                                int64_t n_u, double *v, int64_t n_v, void *stream);
+
 /* ========================================================================= */
 /* Mass operator                                                              */
 /* ========================================================================= */
