@@ -190,7 +190,9 @@ def run_b200(args, rank, world, local_rank):
     ru = fem.Restriction(ne, P**3, 1, N, N, mesh.offsets)
     bu = fem.Basis(3, 1, P, Q)
     op = fem.MassOperator(ru, bu, qdata)
-    launches = op.info()["launches_per_apply"]
+    op.set_kernel(fem.KernelVariant[args.kernel])
+    info = op.info()
+    launches = info["launches_per_apply"]
     del x, rx, bx, qdata
     torch.cuda.synchronize()
     torch.cuda.empty_cache()
@@ -269,7 +271,9 @@ def run_b200(args, rank, world, local_rank):
         "config": {"workload": WORKLOAD, "mesh": "x".join(map(str, SHAPE)), "P": P, "Q": Q, "num_comp": NC,
                    "dofs": N, "elements": ne, "scatter": "atomic", "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (3.3 GB per apply); no flush",
-                   "kernel": "mass3d_apply_kernel<5,6>", "kernel_ms": t_kern,
+                   "kernel": "mass3d_apply_{}kernel<{},{}>".format(
+                       {"pipelined": "pipe_", "paired": "x2_", "prefetch": "prefetch_", "occupancy": "occ_"}.get(info["kernel"], ""), P, Q),
+                   "kernel_variant": info["kernel"], "kernel_ms": t_kern,
                    "algorithmic_bytes_per_apply": abytes,
                    "algorithmic_flops_per_apply": algorithmic_flops(ne, P, Q)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -290,6 +294,104 @@ def run_b200(args, rank, world, local_rank):
     return line
 
 
+# ---------------------------------------------------------------------------
+# order sweep: P = 2..8 (Q = P+1), num_comp 1 and 3, ~64M DoFs, every kernel
+# variant, plus the standalone interp / grad basis applies (extra JSON lines)
+# ---------------------------------------------------------------------------
+def run_sweep(args):
+    import torch
+    import fe_demo_cpp_b200 as fem
+    from fe_demo_cpp_b200.build import build
+    from fe_demo_cpp_b200.mesh import mesh_for_dofs
+    from fe_demo_cpp_b200.mesh_gpu import box_mesh_device
+
+    build()
+    dev = torch.device("cuda", 0)
+    peak, _ = measured_peaks()
+    Ps = [int(p) for p in args.sweep_P.split(",")]
+    for Pp in Ps:
+        Qq = Pp + 1
+        for nc in (1, 3):
+            shape = mesh_for_dofs(64_000_000 // nc, Pp)
+            m = box_mesh_device(shape, Pp, seed=SEED, device=dev)
+            N, ne = m.num_nodes, m.num_elem
+            offs = m.offsets.cpu().numpy()
+            rx = fem.Restriction(ne, Pp**3, 3, N, 3 * N, offs)
+            bx = fem.Basis(3, 3, Pp, Qq)
+            qd = torch.empty(Qq**3 * ne, dtype=torch.float64, device=dev)
+            fem.mass_build(rx, bx, m.coords, qd)
+            del rx, bx
+            m.coords = None
+            ru = fem.Restriction(ne, Pp**3, nc, N, nc * N, offs)
+            bu = fem.Basis(3, nc, Pp, Qq)
+            op = fem.MassOperator(ru, bu, qd, fem.QF.apply_mass_vector if nc > 1 else fem.QF.apply_mass)
+            u = torch.rand(nc * N, dtype=torch.float64, device=dev) * 2 - 1
+            v = torch.empty_like(u)
+            abytes = algorithmic_bytes(ne, N, Pp, Qq, nc)
+            for variant in fem.KernelVariant:
+                if variant == fem.KernelVariant.auto:
+                    continue
+                try:
+                    op.set_kernel(variant)
+                except fem.FemUnsupported:
+                    continue
+                for _ in range(3):
+                    op.apply_add(u, v)
+                torch.cuda.synchronize()
+                t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                t0.record()
+                for _ in range(args.sweep_steps):
+                    op.apply_add(u, v)
+                t1.record()
+                torch.cuda.synchronize()
+                kms = t0.elapsed_time(t1) / args.sweep_steps
+                print(json.dumps({"sweep": "mass_apply", "P": Pp, "Q": Qq, "num_comp": nc, "mesh": list(shape),
+                                  "dofs": nc * N, "kernel": variant.name, "kernel_ms": kms,
+                                  "gdofs_kernel": nc * N / kms / 1e6,
+                                  "roofline_frac": abytes / (kms * 1e-3) / 1e9 / peak,
+                                  "fp64_tflops": algorithmic_flops(ne, Pp, Qq, nc) / (kms * 1e-3) / 1e12}),
+                      flush=True)
+            op.set_kernel(fem.KernelVariant.auto)
+            ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev[0].record()
+            for _ in range(args.sweep_steps):
+                op.apply(u, v)
+            ev[1].record()
+            torch.cuda.synchronize()
+            ams = ev[0].elapsed_time(ev[1]) / args.sweep_steps
+            print(json.dumps({"sweep": "mass_apply_auto", "P": Pp, "Q": Qq, "num_comp": nc, "dofs": nc * N,
+                              "kernel": op.info()["kernel"], "ms_per_apply": ams,
+                              "gdofs": nc * N / ams / 1e6}), flush=True)
+            del op, ru, qd, u, v
+            # standalone basis applies on E-vector / Q-vector sized arrays
+            pn, qn = nc * Pp**3 * ne, nc * Qq**3 * ne
+            if nc == 1:
+                b = fem.Basis(3, nc, Pp, Qq)
+                for name, t_mode, ev_mode, n_in, n_out, flop_mult in [
+                        ("interp", 0, 1, pn, qn, 1), ("interpT", 1, 1, qn, pn, 1),
+                        ("grad", 0, 2, pn, 3 * qn, 3), ("gradT", 1, 2, 3 * qn, pn, 3)]:
+                    x = torch.rand(n_in, dtype=torch.float64, device=dev)
+                    y = torch.empty(n_out, dtype=torch.float64, device=dev)
+                    b.apply(ne, t_mode, ev_mode, x, y)
+                    torch.cuda.synchronize()
+                    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    t0.record()
+                    steps = max(2, args.sweep_steps // 4)
+                    for _ in range(steps):
+                        b.apply(ne, t_mode, ev_mode, x, y)
+                    t1.record()
+                    torch.cuda.synchronize()
+                    ms = t0.elapsed_time(t1) / steps
+                    flops = flop_mult * ne * 2 * (Pp**3 * Qq + Pp**2 * Qq**2 + Pp * Qq**3)
+                    print(json.dumps({"sweep": "basis_apply", "op": name, "P": Pp, "Q": Qq, "elements": ne,
+                                      "ms": ms, "io_gbs": 8 * (n_in + n_out) / (ms * 1e-3) / 1e9,
+                                      "fp64_tflops": flops / (ms * 1e-3) / 1e12}), flush=True)
+                    del x, y
+                b.close()
+            torch.cuda.empty_cache()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -300,7 +402,13 @@ def main():
     ap.add_argument("--cpu-sample-s", type=float, default=12.0, help="approximate CPU seconds of the baseline")
     ap.add_argument("--shape", default=None, help="elements per direction nx,ny,nz (default 100,100,100)")
     ap.add_argument("--P", type=int, default=None, help="nodes per direction (Q = P+1)")
+    ap.add_argument("--kernel", choices=["auto", "simple", "pipelined", "paired", "prefetch", "occupancy"], default="auto")
+    ap.add_argument("--sweep", action="store_true", help="order sweep P=2..8, num_comp 1 and 3 (extra lines)")
+    ap.add_argument("--sweep-P", default="2,3,4,5,6,7,8")
+    ap.add_argument("--sweep-steps", type=int, default=20)
     args = ap.parse_args()
+    if args.sweep:
+        return run_sweep(args)
     global SHAPE, P, Q, WORKLOAD
     if args.shape or args.P:
         SHAPE = tuple(int(s) for s in args.shape.split(",")) if args.shape else SHAPE

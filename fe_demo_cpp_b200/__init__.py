@@ -12,6 +12,7 @@ from .api import (  # noqa: F401
     Basis,
     ContractMode,
     EvalMode,
+    KernelVariant,
     MassOperator,
     QuadMode,
     Restriction,

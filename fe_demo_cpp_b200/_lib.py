@@ -45,7 +45,9 @@ SIGNATURES = {
     "fem_b200_mass_apply": ([_p, _p, _i64, _p, _i64, _p], _i),
     "fem_b200_mass_apply_add": ([_p, _p, _i64, _p, _i64, _p], _i),
     "fem_b200_mass_apply_host": ([_p, _p, _i64, _p, _i64, _p], _i),
-    "fem_b200_mass_info": ([_p, _p, _p, _p], _i),
+    "fem_b200_mass_info": ([_p, _p, _p, _p, _p], _i),
+    "fem_b200_mass_set_kernel": ([_p, _i], _i),
+    "fem_b200_mass_check": ([_p, _p], _i),
 }
 
 _lib = None

@@ -39,6 +39,15 @@ class ScatterMode(IntEnum):
     Deterministic = 1
 
 
+class KernelVariant(IntEnum):
+    auto = 0
+    simple = 1
+    pipelined = 2
+    paired = 3
+    prefetch = 4
+    occupancy = 5
+
+
 class QF(IntEnum):
     """Device QFunctions of the mass operator."""
     apply_mass = 0          # the reference apply_mass: component 0 only
@@ -267,7 +276,16 @@ class MassOperator(_Handle):
         return v
 
     def info(self):
-        launches, tile = C.c_int(0), C.c_int(0)
+        launches, tile, variant = C.c_int(0), C.c_int(0), C.c_int(0)
         nbytes = C.c_int64(0)
-        call("fem_b200_mass_info", self.h, C.addressof(launches), C.addressof(tile), C.addressof(nbytes))
-        return {"launches_per_apply": launches.value, "tile_elems": tile.value, "device_bytes": nbytes.value}
+        call("fem_b200_mass_info", self.h, C.addressof(launches), C.addressof(tile), C.addressof(nbytes),
+             C.addressof(variant))
+        return {"launches_per_apply": launches.value, "tile_elems": tile.value, "device_bytes": nbytes.value,
+                "kernel": KernelVariant(variant.value).name}
+
+    def set_kernel(self, variant) -> None:
+        call("fem_b200_mass_set_kernel", self.h, int(variant))
+
+    def check(self, stream=None) -> None:
+        """Synchronise and raise if a device-side wait of the plan's kernels ran out."""
+        call("fem_b200_mass_check", self.h, _stream(stream))

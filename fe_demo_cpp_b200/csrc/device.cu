@@ -14,6 +14,9 @@
 #include "fem_b200.h"
 #include "host_setup.hpp"
 #include "mass_kernels.cuh"
+#include "mass_pipe.cuh"
+#include "mass_x2.cuh"
+#include "mass_prefetch.cuh"
 #include "restriction_kernels.cuh"
 
 namespace fem_b200 {
@@ -134,7 +137,14 @@ struct MassPlan {
   DevBuf<double> qd_t;
   DevBuf<double> evec;    // deterministic mode: element contributions
   DevBuf<double> hu, hv;  // staging for the host-memory apply
-  ApplyLauncher launch = nullptr;
+  DevBuf<int> status;     // device status word (bit 0: a bounded wait ran out)
+  ApplyLauncher launch = nullptr;       // the kernel in use
+  ApplyLauncher launch_simple = nullptr;
+  ApplyLauncher launch_pipe = nullptr;  // nullptr where the pipelined kernel does not apply
+  ApplyLauncher launch_x2 = nullptr;    // two elements per thread (dim 3)
+  ApplyLauncher launch_pf = nullptr;    // persistent, prefetching (dim 3)
+  ApplyLauncher launch_occ = nullptr;   // one-tile CTAs, register-capped for occupancy (dim 3)
+  int variant = FEM_B200_KERNEL_AUTO;
 };
 
 template <int P, int Q>
@@ -160,13 +170,72 @@ void set_smem(K kernel, int bytes, std::atomic<uint64_t>& done) {
   done.fetch_or(bit);
 }
 
-template <int P, int Q>
+template <int P, int Q, int MINB = 1>
 void launch_apply3(const MassPlan& p, const double* u, double* v, double* ev, cudaStream_t s) {
   using L = Mass3D<P, Q>;
   static std::atomic<uint64_t> smem_set{0};
-  set_smem(mass3d_apply_kernel<P, Q>, L::SMEM, smem_set);
-  mass3d_apply_kernel<P, Q><<<unsigned(p.n_tiles), L::NT, L::SMEM, s>>>(
+  set_smem(mass3d_apply_kernel<P, Q, MINB>, L::SMEM, smem_set);
+  mass3d_apply_kernel<P, Q, MINB><<<unsigned(p.n_tiles), L::NT, L::SMEM, s>>>(
       make_mat<P, Q>(p.basis), p.offs_t.get(), p.qd_t.get(), u, v, ev, p.num_elem, p.comp_run, p.comp_stride);
+  FEM_LAUNCH_CHECK();
+}
+
+// Persistent grid: SMs x resident CTAs (from the occupancy calculator), at
+// most one CTA per tile.
+template <class K>
+int persistent_grid(K kernel, int threads, int smem, int64_t n_tiles) {
+  static std::mutex mu;
+  static int cached[64] = {};
+  const int dev = current_device();
+  int per_grid = 0;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev < 64 && cached[dev]) per_grid = cached[dev];
+  }
+  if (!per_grid) {
+    int sms = 0, blocks = 0;
+    FEM_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    FEM_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, threads, smem));
+    per_grid = sms * std::max(blocks, 1);
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev < 64) cached[dev] = per_grid;
+  }
+  return int(std::min<int64_t>(n_tiles, per_grid));
+}
+
+template <int P, int Q>
+void launch_apply3_pipe(const MassPlan& p, const double* u, double* v, double* ev, cudaStream_t s) {
+  using L = Pipe3D<P, Q>;
+  static std::atomic<uint64_t> smem_set{0};
+  set_smem(mass3d_apply_pipe_kernel<P, Q>, L::SMEM, smem_set);
+  const int grid = persistent_grid(mass3d_apply_pipe_kernel<P, Q>, L::NT, L::SMEM, p.n_tiles);
+  mass3d_apply_pipe_kernel<P, Q><<<grid, L::NT, L::SMEM, s>>>(make_mat<P, Q>(p.basis), p.offs_t.get(),
+                                                               p.qd_t.get(), u, v, ev, p.num_elem, p.comp_run,
+                                                               p.comp_stride, p.n_tiles, p.status.get());
+  FEM_LAUNCH_CHECK();
+}
+
+template <int P, int Q>
+void launch_apply3_pf(const MassPlan& p, const double* u, double* v, double* ev, cudaStream_t s) {
+  using L = Mass3D<P, Q>;
+  constexpr int smem = Prefetch3D<P, Q>::SMEM;
+  static std::atomic<uint64_t> smem_set{0};
+  set_smem(mass3d_apply_prefetch_kernel<P, Q>, smem, smem_set);
+  const int grid = persistent_grid(mass3d_apply_prefetch_kernel<P, Q>, L::NT, smem, p.n_tiles);
+  mass3d_apply_prefetch_kernel<P, Q><<<grid, L::NT, smem, s>>>(make_mat<P, Q>(p.basis), p.offs_t.get(),
+                                                                p.qd_t.get(), u, v, ev, p.num_elem, p.comp_run,
+                                                                p.comp_stride, int(p.n_tiles), p.status.get());
+  FEM_LAUNCH_CHECK();
+}
+
+template <int P, int Q>
+void launch_apply3_x2(const MassPlan& p, const double* u, double* v, double* ev, cudaStream_t s) {
+  using L = Mass3DX2<P, Q>;
+  static std::atomic<uint64_t> smem_set{0};
+  set_smem(mass3d_apply_x2_kernel<P, Q>, L::SMEM, smem_set);
+  const unsigned grid = unsigned((p.n_tiles + 1) / 2);  // the plan's tile arrays hold an even number of tiles
+  mass3d_apply_x2_kernel<P, Q><<<grid, L::NT, L::SMEM, s>>>(make_mat<P, Q>(p.basis), p.offs_t.get(), p.qd_t.get(),
+                                                             u, v, ev, p.num_elem, p.comp_run, p.comp_stride);
   FEM_LAUNCH_CHECK();
 }
 
@@ -221,31 +290,44 @@ constexpr int kMinP = 2, kMaxP = 8, kQSpan = 3;
 
 template <int P, int DQ>
 struct Table {
-  static void fill(ApplyLauncher (*ap)[kMaxP + 1][kQSpan], BuildLauncher (*bd)[kMaxP + 1][kQSpan]) {
+  static void fill(ApplyLauncher (*ap)[kMaxP + 1][kQSpan], BuildLauncher (*bd)[kMaxP + 1][kQSpan],
+                   ApplyLauncher (*pp)[kQSpan], ApplyLauncher (*xx)[kQSpan], ApplyLauncher (*pf)[kQSpan],
+                   ApplyLauncher (*oc)[kQSpan]) {
     constexpr int Q = P + DQ;
     ap[0][P][DQ] = launch_apply1<P, Q>;
     ap[1][P][DQ] = launch_apply2<P, Q>;
     ap[2][P][DQ] = launch_apply3<P, Q>;
+    if constexpr (Pipe3D<P, Q>::SMEM <= kMaxSmemPerCta) pp[P][DQ] = launch_apply3_pipe<P, Q>;
+    if constexpr (Mass3DX2<P, Q>::SMEM <= kMaxSmemPerCta && Mass3DX2<P, Q>::NT <= 1024) xx[P][DQ] = launch_apply3_x2<P, Q>;
+    if constexpr (Prefetch3D<P, Q>::SMEM <= kMaxSmemPerCta) pf[P][DQ] = launch_apply3_pf<P, Q>;
+    if constexpr (Mass3D<P, Q>::MINB_OCC > 1) oc[P][DQ] = launch_apply3<P, Q, Mass3D<P, Q>::MINB_OCC>;
     bd[0][P][DQ] = launch_build1<P, Q>;
     bd[1][P][DQ] = launch_build2<P, Q>;
     bd[2][P][DQ] = launch_build3<P, Q>;
     if constexpr (DQ + 1 < kQSpan)
-      Table<P, DQ + 1>::fill(ap, bd);
+      Table<P, DQ + 1>::fill(ap, bd, pp, xx, pf, oc);
     else if constexpr (P + 1 <= kMaxP)
-      Table<P + 1, 0>::fill(ap, bd);
+      Table<P + 1, 0>::fill(ap, bd, pp, xx, pf, oc);
   }
 };
 
 struct Dispatch {
   ApplyLauncher apply[3][kMaxP + 1][kQSpan] = {};
   BuildLauncher build[3][kMaxP + 1][kQSpan] = {};
-  Dispatch() { Table<kMinP, 0>::fill(apply, build); }
+  ApplyLauncher apply3_pipe[kMaxP + 1][kQSpan] = {};
+  ApplyLauncher apply3_x2[kMaxP + 1][kQSpan] = {};
+  ApplyLauncher apply3_pf[kMaxP + 1][kQSpan] = {};
+  ApplyLauncher apply3_occ[kMaxP + 1][kQSpan] = {};
+  Dispatch() { Table<kMinP, 0>::fill(apply, build, apply3_pipe, apply3_x2, apply3_pf, apply3_occ); }
 };
 
 const Dispatch& dispatch() {
   static Dispatch d;
   return d;
 }
+
+// The variant FEM_B200_KERNEL_AUTO selects for a plan.
+ApplyLauncher auto_kernel(const MassPlan& p) { return p.launch_simple; }
 
 bool fused_supported(int dim, int P, int Q) {
   return dim >= 1 && dim <= 3 && P >= kMinP && P <= kMaxP && Q >= P && Q < P + kQSpan;
@@ -708,7 +790,8 @@ int fem_b200_mass_create(fem_b200_restriction ru, fem_b200_basis bu, const doubl
     p->r = r;
     p->tile_e = b.dim == 3 ? 8 : (b.dim == 2 ? 32 : 128);
     p->n_tiles = (int64_t(p->num_elem) + p->tile_e - 1) / p->tile_e;
-    const int64_t ne_pad = p->n_tiles * p->tile_e;
+    // an even number of tiles, so a kernel taking two tiles per CTA stays inside
+    const int64_t ne_pad = ((p->n_tiles + 1) / 2) * 2 * p->tile_e;
     p->offs_t.alloc(size_t(ne_pad * p->es));
     p->qd_t.alloc(size_t(ne_pad * p->nq));
     tile_offsets_kernel<<<grid_for(ne_pad * p->es, 256), 256>>>(r->offsets.get(), p->num_elem, p->es, p->tile_e,
@@ -718,7 +801,14 @@ int fem_b200_mass_create(fem_b200_restriction ru, fem_b200_basis bu, const doubl
                                                               ne_pad * p->nq, p->qd_t.get());
     FEM_LAUNCH_CHECK();
     if (p->scatter_mode == FEM_B200_SCATTER_DETERMINISTIC) p->evec.alloc(size_t(int64_t(p->comp_run) * p->es * p->num_elem));
-    p->launch = dispatch().apply[b.dim - 1][b.P][b.Q - b.P];
+    p->status.alloc(1);
+    FEM_CUDA_CHECK(cudaMemset(p->status.get(), 0, sizeof(int)));
+    p->launch_simple = dispatch().apply[b.dim - 1][b.P][b.Q - b.P];
+    p->launch_pipe = b.dim == 3 ? dispatch().apply3_pipe[b.P][b.Q - b.P] : nullptr;
+    p->launch_x2 = b.dim == 3 ? dispatch().apply3_x2[b.P][b.Q - b.P] : nullptr;
+    p->launch_pf = b.dim == 3 ? dispatch().apply3_pf[b.P][b.Q - b.P] : nullptr;
+    p->launch_occ = b.dim == 3 ? dispatch().apply3_occ[b.P][b.Q - b.P] : nullptr;
+    p->launch = auto_kernel(*p);
     FEM_CUDA_CHECK(cudaDeviceSynchronize());
     *out = new fem_b200_mass_s{std::move(p)};
   });
@@ -729,6 +819,17 @@ int fem_b200_mass_destroy(fem_b200_mass op) {
 }
 
 namespace {
+// Reads and clears the plan's device status word (the caller has synchronised).
+void check_status(MassPlan& p) {
+  int st = 0;
+  FEM_CUDA_CHECK(cudaMemcpy(&st, p.status.get(), sizeof(int), cudaMemcpyDeviceToHost));
+  if (st) {
+    FEM_CUDA_CHECK(cudaMemset(p.status.get(), 0, sizeof(int)));
+    throw cuda_error("operator_apply: a bounded wait in the mass kernel ran out (status " + std::to_string(st) +
+                     "); the result is not valid");
+  }
+}
+
 void mass_apply_impl(MassPlan& p, const double* u, double* v, bool zero, cudaStream_t s) {
   if (zero) FEM_CUDA_CHECK(cudaMemsetAsync(v, 0, size_t(p.l_size) * sizeof(double), s));
   if (p.scatter_mode == FEM_B200_SCATTER_ATOMIC) {
@@ -782,14 +883,57 @@ int fem_b200_mass_apply_host(fem_b200_mass op, const double* u_host, int64_t n_u
     mass_apply_impl(p, p.hu.get(), p.hv.get(), true, s);
     FEM_CUDA_CHECK(cudaMemcpyAsync(v_host, p.hv.get(), bytes, cudaMemcpyDeviceToHost, s));
     FEM_CUDA_CHECK(cudaStreamSynchronize(s));
+    check_status(p);
   });
 }
 
-int fem_b200_mass_info(fem_b200_mass op, int* launches_per_apply, int* tile_elems, int64_t* device_bytes) {
+int fem_b200_mass_check(fem_b200_mass op, void* stream) {
+  return guarded([&] {
+    require(op && op->d, "operator check: NULL handle");
+    MassPlan& p = *op->d;
+    DeviceGuard g(p.device);
+    FEM_CUDA_CHECK(cudaStreamSynchronize(as_stream(stream)));
+    check_status(p);
+  });
+}
+
+int fem_b200_mass_set_kernel(fem_b200_mass op, int variant) {
+  return guarded([&] {
+    require(op && op->d, "operator kernel: NULL handle");
+    MassPlan& p = *op->d;
+    require(variant >= FEM_B200_KERNEL_AUTO && variant <= FEM_B200_KERNEL_OCCUPANCY, "operator kernel: unknown variant");
+    if (variant == FEM_B200_KERNEL_OCCUPANCY && !p.launch_occ)
+      throw unsupported_error("operator kernel: no register-capped kernel for " + shape_str(p.dim, p.P, p.Q));
+    if (variant == FEM_B200_KERNEL_PREFETCH && !p.launch_pf)
+      throw unsupported_error("operator kernel: no prefetching kernel for " + shape_str(p.dim, p.P, p.Q));
+    if (variant == FEM_B200_KERNEL_PIPELINED && !p.launch_pipe)
+      throw unsupported_error("operator kernel: no pipelined kernel for " + shape_str(p.dim, p.P, p.Q));
+    if (variant == FEM_B200_KERNEL_PAIRED && !p.launch_x2)
+      throw unsupported_error("operator kernel: no paired kernel for " + shape_str(p.dim, p.P, p.Q));
+    p.variant = variant;
+    switch (variant) {
+      case FEM_B200_KERNEL_SIMPLE: p.launch = p.launch_simple; break;
+      case FEM_B200_KERNEL_PIPELINED: p.launch = p.launch_pipe; break;
+      case FEM_B200_KERNEL_PAIRED: p.launch = p.launch_x2; break;
+      case FEM_B200_KERNEL_PREFETCH: p.launch = p.launch_pf; break;
+      case FEM_B200_KERNEL_OCCUPANCY: p.launch = p.launch_occ; break;
+      default: p.launch = auto_kernel(p);
+    }
+  });
+}
+
+int fem_b200_mass_info(fem_b200_mass op, int* launches_per_apply, int* tile_elems, int64_t* device_bytes,
+                       int* kernel_variant) {
   return guarded([&] {
     require(op && op->d, "mass info: NULL handle");
     const MassPlan& p = *op->d;
     if (launches_per_apply) *launches_per_apply = p.scatter_mode == FEM_B200_SCATTER_ATOMIC ? 1 : 2;
+    if (kernel_variant)
+      *kernel_variant = p.launch == p.launch_x2     ? FEM_B200_KERNEL_PAIRED
+                        : p.launch == p.launch_pipe ? FEM_B200_KERNEL_PIPELINED
+                        : p.launch == p.launch_pf   ? FEM_B200_KERNEL_PREFETCH
+                        : p.launch == p.launch_occ  ? FEM_B200_KERNEL_OCCUPANCY
+                                                    : FEM_B200_KERNEL_SIMPLE;
     if (tile_elems) *tile_elems = p.tile_e;
     if (device_bytes)
       *device_bytes = int64_t(p.offs_t.bytes() + p.qd_t.bytes() + p.evec.bytes() + p.hu.bytes() + p.hv.bytes());

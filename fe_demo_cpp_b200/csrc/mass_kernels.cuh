@@ -92,6 +92,11 @@ struct Mass3D {
   static constexpr int SB = cmax(P * PS2, Q * PS4);
   static constexpr int SMEM = (SA + SB) * 8;
   static constexpr int ES = P * P * P, NQ = Q * Q * Q;
+  // resident CTAs per SM the register-capped variant asks for: 5, or what
+  // shared memory (227 KB) and threads (2048) allow
+  static constexpr int MINB_OCC = cmax(1, (5 < 232448 / SMEM ? 5 : 232448 / SMEM) < 2048 / NT
+                                              ? (5 < 232448 / SMEM ? 5 : 232448 / SMEM)
+                                              : 2048 / NT);
 };
 
 // num_comp_run components are processed (1 for the reference apply_mass,
@@ -99,8 +104,10 @@ struct Mass3D {
 // ev == nullptr: atomic scatter-add into v.  ev != nullptr: the element
 // contributions are stored in the E-vector layout [k][i][e] (deterministic
 // mode; a transpose-map reduction follows).
-template <int P, int Q>
-__global__ void __launch_bounds__(Mass3D<P, Q>::NT) mass3d_apply_kernel(
+// MINB > 1 asks for MINB resident CTAs per SM (a register cap), trading a
+// little spilling for more warps to hide memory latency.
+template <int P, int Q, int MINB = 1>
+__global__ void __launch_bounds__(Mass3D<P, Q>::NT, MINB) mass3d_apply_kernel(
     const __grid_constant__ Mat1D<P, Q> m, const int* __restrict__ offs, const double* __restrict__ qd,
     const double* __restrict__ u, double* __restrict__ v, double* __restrict__ ev, int num_elem, int num_comp_run,
     int64_t comp_stride) {

@@ -56,6 +56,13 @@ extern "C" {
 /* Device QFunctions (the host side matches fem::qfunctions by pointer) */
 #define FEM_B200_QF_APPLY_MASS 0        /* include/qfunctions/mass.hpp:45-51: component 0 only */
 #define FEM_B200_QF_APPLY_MASS_VECTOR 1 /* every component: v_k = qdata * u_k (no reference counterpart) */
+/* Kernel variants of the fused 3D mass apply (fem_b200_mass_set_kernel) */
+#define FEM_B200_KERNEL_AUTO 0      /* the fastest measured variant for the shape */
+#define FEM_B200_KERNEL_SIMPLE 1    /* one CTA per 8-element tile, one element per thread */
+#define FEM_B200_KERNEL_PIPELINED 2 /* persistent CTAs, next tile staged by bulk copies during this one */
+#define FEM_B200_KERNEL_PAIRED 3    /* one CTA per 16 elements, two adjacent elements per thread */
+#define FEM_B200_KERNEL_PREFETCH 4  /* persistent CTAs, qdata bulk-copied two tiles ahead, offsets/u one ahead */
+#define FEM_B200_KERNEL_OCCUPANCY 5 /* as SIMPLE, registers capped for up to 5 resident CTAs per SM */
 
 typedef struct fem_b200_restriction_s *fem_b200_restriction;
 typedef struct fem_b200_basis_s *fem_b200_basis;
@@ -217,9 +224,21 @@ int fem_b200_mass_apply_add(fem_b200_mass op, const double *u, int64_t n_u, doub
 int fem_b200_mass_apply_host(fem_b200_mass op, const double *u_host, int64_t n_u, double *v_host, int64_t n_v,
                              void *stream);
 
-/* Number of kernel launches one fem_b200_mass_apply makes, and the plan's
- * element-tile size and device footprint in bytes (any pointer may be NULL). */
-int fem_b200_mass_info(fem_b200_mass op, int *launches_per_apply, int *tile_elems, int64_t *device_bytes);
+/* Number of kernel launches one fem_b200_mass_apply makes, the plan's
+ * element-tile size, device footprint in bytes and the kernel variant in use
+ * (any pointer may be NULL). */
+int fem_b200_mass_info(fem_b200_mass op, int *launches_per_apply, int *tile_elems, int64_t *device_bytes,
+                       int *kernel_variant);
+
+/* Select the fused kernel variant (FEM_B200_KERNEL_*).  PIPELINED and PAIRED
+ * are dim-3 kernels; each is FEM_B200_ERROR_UNSUPPORTED where its shared
+ * memory or thread count does not fit a CTA. */
+int fem_b200_mass_set_kernel(fem_b200_mass op, int variant);
+
+/* Synchronise `stream` and report a device-side failure of the plan's kernels
+ * (a bounded wait that ran out) as FEM_B200_ERROR_CUDA.  fem_b200_mass_apply_host
+ * does this check itself. */
+int fem_b200_mass_check(fem_b200_mass op, void *stream);
 
 #ifdef __cplusplus
 }

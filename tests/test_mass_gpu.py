@@ -79,19 +79,25 @@ def test_build_qdata_matches_oracle(fem, cuda, orc, dim, shape, P, Q):
     close(qd, want, TOL * max(shape))
 
 
+@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5], ids=["simple", "pipelined", "paired", "prefetch", "occupancy"])
 @pytest.mark.parametrize("scatter", [0, 1], ids=["atomic", "deterministic"])
 @pytest.mark.parametrize("dim,shape,P,Q", SHAPES)
-def test_apply_matches_oracle(fem, cuda, orc, dim, shape, P, Q, scatter):
+def test_apply_matches_oracle(fem, cuda, orc, dim, shape, P, Q, scatter, variant):
     import torch
+    if variant in (2, 3, 4, 5) and dim != 3:
+        pytest.skip("the pipelined, paired, prefetching and occupancy kernels are 3D only")
     m = _mesh(dim, shape, P, seed=5)
     qd = build_qdata(fem, cuda, m, Q)
     qd_h = host(qd)
     ru = fem.Restriction(m.num_elem, P**dim, 1, m.num_nodes, m.num_nodes, m.offsets, scatter)
     bu = fem.Basis(dim, 1, P, Q)
     op = fem.MassOperator(ru, bu, qd)
+    op.set_kernel(variant)
+    assert op.info()["kernel"] == fem.KernelVariant(variant).name
     u = random_vector(m.num_nodes, 6)
     v = torch.full((m.num_nodes,), 7.0, dtype=torch.float64, device=cuda)  # garbage: apply overwrites
     op.apply(dev(u, cuda), v)
+    op.check()
     want = orc.mass_apply(dim, m.num_elem, P, Q, 1, m.num_nodes, m.num_nodes, m.offsets, qd_h, u)
     close(host(v), want)
 
@@ -107,8 +113,10 @@ def test_three_components(fem, cuda, orc, P, Q, interleaved):
     u = random_vector(l_size, 8)
     ru = fem.Restriction(m.num_elem, P**3, 3, cs, l_size, offs)
     bu = fem.Basis(3, 3, P, Q)
-    for qf, vector in ((fem.QF.apply_mass_vector, True), (fem.QF.apply_mass, False)):
+    for (qf, vector), variant in [(q, k) for q in ((fem.QF.apply_mass_vector, True), (fem.QF.apply_mass, False))
+                                  for k in (1, 2, 3, 4, 5)]:
         op = fem.MassOperator(ru, bu, qd, qf)
+        op.set_kernel(variant)
         v = torch.empty(l_size, dtype=torch.float64, device=cuda)
         op.apply(dev(u, cuda), v)
         want = orc.mass_apply(3, m.num_elem, P, Q, 3, cs, l_size, offs, qd_h, u, vector=vector)
@@ -182,6 +190,39 @@ def test_tail_tiles_and_single_element(fem, cuda, orc):
         v = torch.empty(m.num_nodes, dtype=torch.float64, device=cuda)
         op.apply(dev(u, cuda), v)
         close(host(v), orc.mass_apply(3, m.num_elem, 4, 5, 1, m.num_nodes, m.num_nodes, m.offsets, host(qd), u))
+
+
+@pytest.mark.parametrize("P,Q", [(4, 5), (5, 6), (6, 7)])
+def test_pipelined_equals_simple_on_many_tiles(fem, cuda, P, Q):
+    """Several tiles per persistent CTA (a mesh larger than one wave), the
+    deterministic mode so the two kernels' outputs compare bitwise."""
+    import torch
+    m = box_mesh((40, 30, 20), P, seed=8)
+    qd = build_qdata(fem, cuda, m, Q)
+    op = fem.MassOperator(fem.Restriction(m.num_elem, P**3, 1, m.num_nodes, m.num_nodes, m.offsets, 1),
+                          fem.Basis(3, 1, P, Q), qd)
+    u = dev(random_vector(m.num_nodes, 2), cuda)
+    out = {}
+    for variant in (1, 2, 3, 4, 5):
+        op.set_kernel(variant)
+        v = torch.empty(m.num_nodes, dtype=torch.float64, device=cuda)
+        op.apply(u, v)
+        op.check()
+        out[variant] = host(v)
+    assert np.array_equal(out[1], out[2])
+    assert np.array_equal(out[1], out[3])
+    assert np.array_equal(out[1], out[4])
+    assert np.array_equal(out[1], out[5])
+
+
+def test_pipelined_unavailable_where_smem_does_not_fit(fem, cuda):
+    import torch
+    m = box_mesh((1, 1, 1), 8, seed=0)
+    op = fem.MassOperator(fem.Restriction(1, 512, 1, m.num_nodes, m.num_nodes, m.offsets), fem.Basis(3, 1, 8, 10),
+                          torch.zeros(1000, dtype=torch.float64, device=cuda))
+    assert op.info()["kernel"] in ("simple", "paired")
+    with pytest.raises(fem.FemUnsupported):
+        op.set_kernel(2)
 
 
 def test_unsupported_shape_fails_loudly(fem, cuda):
