@@ -36,9 +36,23 @@ SIGNATURES = {
     "fem_b200_restriction_apply": ([_p, _i, _p, _i64, _p, _i64, _p], _i),
     "fem_b200_restriction_multiplicity": ([_p, _p, _i64, _p], _i),
     "fem_b200_basis_create": ([_i, _i, _i, _i, _i, _p], _i),
+    "fem_b200_basis_create_from": ([_i, _i, _i, _i, _p, _p, _p, _p], _i),
     "fem_b200_basis_destroy": ([_p], _i),
     "fem_b200_basis_apply": ([_p, _i, _i, _i, _p, _i64, _p, _i64, _p], _i),
     "fem_b200_basis_apply_static": ([_p, _i, _i, _i, _p, _i64, _p, _i64, _p], _i),
+    "fem_b200_malloc": ([_p, C.c_size_t], _i),
+    "fem_b200_free": ([_p], _i),
+    "fem_b200_memcpy": ([_p, _p, C.c_size_t, _i, _p], _i),
+    "fem_b200_memset_zero": ([_p, C.c_size_t, _p], _i),
+    "fem_b200_synchronize": ([_p], _i),
+    "fem_b200_device_info": ([_i, _p, _i, _p, _p], _i),
+    "fem_b200_offset_gather": ([_i, _i, _i, _i, _p, _p, _p, _p], _i),
+    "fem_b200_offset_scatter_add": ([_i, _i, _i, _i, _p, _p, _p, _p], _i),
+    "fem_b200_transpose_scatter_add": ([_i, _i, _i, _i, _i, _p, _p, _p, _p, _p, _p], _i),
+    "fem_b200_strided_apply": ([_i, _i, _i, _i, _p, _p, _p, _p], _i),
+    "fem_b200_contract": ([_i64, _i, _i64, _i, _p, _i, _i, _p, _p, _p], _i),
+    "fem_b200_qfunction_apply_mass": ([_i64, _p, _p, _p, _p], _i),
+    "fem_b200_qfunction_build_mass": ([_i, _i64, _p, _p, _p, _p], _i),
     "fem_b200_mass_build": ([_p, _p, _p, _i64, _p, _i64, _p], _i),
     "fem_b200_mass_create": ([_p, _p, _p, _i64, _i, _p], _i),
     "fem_b200_mass_destroy": ([_p], _i),
@@ -48,6 +62,7 @@ SIGNATURES = {
     "fem_b200_mass_info": ([_p, _p, _p, _p, _p], _i),
     "fem_b200_mass_set_kernel": ([_p, _i], _i),
     "fem_b200_mass_check": ([_p, _p], _i),
+    "fem_b200_mass_autotune": ([_p, _p, _i64, _p, _i64, _i, _p, _p, _p], _i),
 }
 
 _lib = None

@@ -286,6 +286,16 @@ class MassOperator(_Handle):
     def set_kernel(self, variant) -> None:
         call("fem_b200_mass_set_kernel", self.h, int(variant))
 
+    def autotune(self, u, v, reps: int = 10, stream=None):
+        """Time every kernel variant on (u, v) (v is scratch), keep the fastest;
+        returns (variant name, ms per apply)."""
+        _check_dev(u)
+        _check_dev(v)
+        chosen, ms = C.c_int(0), C.c_float(0.0)
+        call("fem_b200_mass_autotune", self.h, _ptr(u), _n(u), _ptr(v), _n(v), int(reps), C.addressof(chosen),
+             C.addressof(ms), _stream(stream))
+        return KernelVariant(chosen.value).name, ms.value
+
     def check(self, stream=None) -> None:
         """Synchronise and raise if a device-side wait of the plan's kernels ran out."""
         call("fem_b200_mass_check", self.h, _stream(stream))

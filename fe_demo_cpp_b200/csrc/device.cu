@@ -4,6 +4,8 @@
 
 #include <algorithm>
 #include <atomic>
+#include <map>
+#include <tuple>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -326,8 +328,49 @@ const Dispatch& dispatch() {
   return d;
 }
 
-// The variant FEM_B200_KERNEL_AUTO selects for a plan.
-ApplyLauncher auto_kernel(const MassPlan& p) { return p.launch_simple; }
+// ---------------------------------------------------------------------------
+// Autotuner: which variant ran fastest for a (device, dim, P, Q, components,
+// scatter mode, size class).  Filled by fem_b200_mass_autotune; consulted by
+// FEM_B200_KERNEL_AUTO when a plan is created or reset to AUTO.
+// ---------------------------------------------------------------------------
+struct TuneKey {
+  int device, dim, P, Q, comp_run, scatter, size_class;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(device, dim, P, Q, comp_run, scatter, size_class) <
+           std::tie(o.device, o.dim, o.P, o.Q, o.comp_run, o.scatter, o.size_class);
+  }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, int> g_tune;
+
+TuneKey tune_key(const MassPlan& p) {
+  int size_class = 0;
+  for (int64_t n = p.num_elem; n > 1; n >>= 1) ++size_class;  // log2(num_elem)
+  return {p.device, p.dim, p.P, p.Q, p.comp_run, p.scatter_mode, size_class};
+}
+
+ApplyLauncher variant_launcher(const MassPlan& p, int variant) {
+  switch (variant) {
+    case FEM_B200_KERNEL_SIMPLE: return p.launch_simple;
+    case FEM_B200_KERNEL_PIPELINED: return p.launch_pipe;
+    case FEM_B200_KERNEL_PAIRED: return p.launch_x2;
+    case FEM_B200_KERNEL_PREFETCH: return p.launch_pf;
+    case FEM_B200_KERNEL_OCCUPANCY: return p.launch_occ;
+    default: return nullptr;
+  }
+}
+
+// The variant FEM_B200_KERNEL_AUTO selects for a plan: the autotuned choice
+// for its key if there is one, else the one-tile kernel.
+ApplyLauncher auto_kernel(const MassPlan& p) {
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  auto it = g_tune.find(tune_key(p));
+  if (it != g_tune.end()) {
+    ApplyLauncher l = variant_launcher(p, it->second);
+    if (l) return l;
+  }
+  return p.launch_simple;
+}
 
 bool fused_supported(int dim, int P, int Q) {
   return dim >= 1 && dim <= 3 && P >= kMinP && P <= kMaxP && Q >= P && Q < P + kQSpan;
@@ -628,6 +671,29 @@ int fem_b200_basis_create(int dim, int num_comp, int P, int Q, int quad_mode, fe
   });
 }
 
+int fem_b200_basis_create_from(int dim, int num_comp, int P, int Q, const double* q_weight, const double* interp,
+                               const double* grad, fem_b200_basis* out) {
+  return guarded([&] {
+    require(out != nullptr, "basis: NULL output handle");
+    require(dim >= 1 && dim <= 3 && num_comp >= 1 && P >= 1 && Q >= 1, "basis: bad sizes");
+    require(q_weight && interp && grad, "basis: NULL matrix");
+    auto d = std::make_unique<BasisDev>();
+    d->h.dim = dim, d->h.num_comp = num_comp, d->h.P = P, d->h.Q = Q, d->h.quad_mode = -1;
+    d->h.q_ref.assign(size_t(Q), 0.0);
+    d->h.q_weight.assign(q_weight, q_weight + Q);
+    d->h.interp.assign(interp, interp + size_t(Q) * P);
+    d->h.grad.assign(grad, grad + size_t(Q) * P);
+    d->device = current_device();
+    d->interp.alloc(d->h.interp.size());
+    d->grad.alloc(d->h.grad.size());
+    d->weight.alloc(d->h.q_weight.size());
+    FEM_CUDA_CHECK(cudaMemcpy(d->interp.get(), d->h.interp.data(), d->interp.bytes(), cudaMemcpyHostToDevice));
+    FEM_CUDA_CHECK(cudaMemcpy(d->grad.get(), d->h.grad.data(), d->grad.bytes(), cudaMemcpyHostToDevice));
+    FEM_CUDA_CHECK(cudaMemcpy(d->weight.get(), d->h.q_weight.data(), d->weight.bytes(), cudaMemcpyHostToDevice));
+    *out = new fem_b200_basis_s{std::move(d)};
+  });
+}
+
 int fem_b200_basis_destroy(fem_b200_basis b) {
   return guarded([&] { delete b; });
 }
@@ -738,6 +804,152 @@ int fem_b200_basis_apply_static(fem_b200_basis b, int num_elem, int t_mode, int 
         post *= Q;
       }
     }
+  });
+}
+
+// ---- device memory and raw launchers (the C++ drop-in's building blocks) ----
+int fem_b200_malloc(void** ptr, size_t bytes) {
+  return guarded([&] {
+    require(ptr != nullptr, "fem_b200_malloc: NULL output");
+    *ptr = nullptr;
+    if (bytes) FEM_CUDA_CHECK(cudaMalloc(ptr, bytes));
+  });
+}
+
+int fem_b200_free(void* ptr) {
+  return guarded([&] {
+    if (ptr) FEM_CUDA_CHECK(cudaFree(ptr));
+  });
+}
+
+int fem_b200_memcpy(void* dst, const void* src, size_t bytes, int kind, void* stream) {
+  return guarded([&] {
+    require(kind >= 0 && kind <= 2, "fem_b200_memcpy: kind must be 0 (H2D), 1 (D2H) or 2 (D2D)");
+    if (!bytes) return;
+    require(dst && src, "fem_b200_memcpy: NULL pointer");
+    const cudaMemcpyKind k[3] = {cudaMemcpyHostToDevice, cudaMemcpyDeviceToHost, cudaMemcpyDeviceToDevice};
+    cudaStream_t s = as_stream(stream);
+    FEM_CUDA_CHECK(cudaMemcpyAsync(dst, src, bytes, k[kind], s));
+    if (kind != 2) FEM_CUDA_CHECK(cudaStreamSynchronize(s));
+  });
+}
+
+int fem_b200_memset_zero(void* ptr, size_t bytes, void* stream) {
+  return guarded([&] {
+    if (bytes) FEM_CUDA_CHECK(cudaMemsetAsync(ptr, 0, bytes, as_stream(stream)));
+  });
+}
+
+int fem_b200_synchronize(void* stream) {
+  return guarded([&] { FEM_CUDA_CHECK(cudaStreamSynchronize(as_stream(stream))); });
+}
+
+int fem_b200_device_info(int device, char* name, int name_len, int* ints, int64_t* sizes) {
+  return guarded([&] {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+      (void)cudaGetLastError();
+      n = 0;
+    }
+    require(device >= 0 && device < n, "device_info: no such CUDA device");
+    cudaDeviceProp prop;
+    FEM_CUDA_CHECK(cudaGetDeviceProperties(&prop, device));
+    if (name && name_len > 0) {
+      std::strncpy(name, prop.name, size_t(name_len) - 1);
+      name[name_len - 1] = '\0';
+    }
+    if (ints) {
+      ints[0] = prop.major, ints[1] = prop.minor, ints[2] = prop.multiProcessorCount, ints[3] = prop.warpSize;
+      ints[4] = prop.maxThreadsPerBlock, ints[5] = prop.regsPerBlock;
+    }
+    if (sizes) {
+      DeviceGuard g(device);
+      size_t free_b = 0, total_b = 0;
+      FEM_CUDA_CHECK(cudaMemGetInfo(&free_b, &total_b));
+      sizes[0] = int64_t(prop.sharedMemPerBlock), sizes[1] = int64_t(prop.sharedMemPerBlockOptin);
+      sizes[2] = int64_t(prop.sharedMemPerMultiprocessor), sizes[3] = int64_t(prop.totalGlobalMem);
+      sizes[4] = int64_t(free_b);
+    }
+  });
+}
+
+int fem_b200_offset_gather(int num_elem, int elem_size, int num_comp, int comp_stride, const int* offsets,
+                           const double* l_in, double* e_out, void* stream) {
+  return guarded([&] {
+    require(num_elem > 0 && elem_size > 0 && num_comp > 0 && offsets && l_in && e_out, "offset gather: bad arguments");
+    const dim3 grid(unsigned((elem_size + kTile - 1) / kTile), unsigned((num_elem + kTile - 1) / kTile));
+    offset_tile_kernel<0><<<grid, dim3(kTile, 8), 0, as_stream(stream)>>>(offsets, num_elem, elem_size, num_comp,
+                                                                         comp_stride, l_in, e_out);
+    FEM_LAUNCH_CHECK();
+  });
+}
+
+int fem_b200_offset_scatter_add(int num_elem, int elem_size, int num_comp, int comp_stride, const int* offsets,
+                                const double* e_in, double* l_out, void* stream) {
+  return guarded([&] {
+    require(num_elem > 0 && elem_size > 0 && num_comp > 0 && offsets && e_in && l_out, "offset scatter: bad arguments");
+    const dim3 grid(unsigned((elem_size + kTile - 1) / kTile), unsigned((num_elem + kTile - 1) / kTile));
+    offset_tile_kernel<1><<<grid, dim3(kTile, 8), 0, as_stream(stream)>>>(offsets, num_elem, elem_size, num_comp,
+                                                                         comp_stride, e_in, l_out);
+    FEM_LAUNCH_CHECK();
+  });
+}
+
+int fem_b200_transpose_scatter_add(int num_nodes, int num_elem, int elem_size, int num_comp, int comp_stride,
+                                   const int* l_vec_indices, const int* t_offsets, const int* t_indices,
+                                   const double* e_in, double* l_out, void* stream) {
+  return guarded([&] {
+    require(num_nodes >= 0 && num_elem > 0 && elem_size > 0 && num_comp > 0, "transpose scatter: bad sizes");
+    if (num_nodes == 0) return;
+    require(l_vec_indices && t_offsets && t_indices && e_in && l_out, "transpose scatter: NULL array");
+    csr_scatter_kernel<<<grid_for(num_nodes, 256), 256, 0, as_stream(stream)>>>(
+        num_nodes, num_elem, elem_size, num_comp, comp_stride, l_vec_indices, t_offsets, t_indices, e_in, l_out);
+    FEM_LAUNCH_CHECK();
+  });
+}
+
+int fem_b200_strided_apply(int t_mode, int num_elem, int elem_size, int num_comp, const int* strides,
+                           const double* in, double* out, void* stream) {
+  return guarded([&] {
+    require(num_elem > 0 && elem_size > 0 && num_comp > 0 && strides && in && out, "strided apply: bad arguments");
+    const int64_t n = int64_t(num_elem) * elem_size * num_comp;
+    if (t_mode == FEM_B200_NOTRANSPOSE)
+      strided_kernel<0><<<grid_for(n, 256), 256, 0, as_stream(stream)>>>(num_elem, elem_size, num_comp, strides[0],
+                                                                         strides[1], strides[2], in, out);
+    else
+      strided_kernel<1><<<grid_for(n, 256), 256, 0, as_stream(stream)>>>(num_elem, elem_size, num_comp, strides[0],
+                                                                         strides[1], strides[2], in, out);
+    FEM_LAUNCH_CHECK();
+  });
+}
+
+int fem_b200_contract(int64_t A, int B, int64_t C, int J, const double* t, int t_mode, int add, const double* u,
+                      double* v, void* stream) {
+  return guarded([&] {
+    require(A >= 0 && B >= 0 && C >= 0 && J >= 0, "tensor_contract_apply: negative size");
+    const int64_t n = A * J * C;
+    if (n == 0) return;
+    require(t && u && v, "tensor_contract_apply: NULL array");
+    contract_kernel<<<grid_for(n, 256), 256, 0, as_stream(stream)>>>(A, B, C, J, t, t_mode == FEM_B200_TRANSPOSE,
+                                                                     add ? 1 : 0, u, v);
+    FEM_LAUNCH_CHECK();
+  });
+}
+
+int fem_b200_qfunction_apply_mass(int64_t Q, const double* u, const double* qdata, double* v, void* stream) {
+  return guarded([&] {
+    require(Q > 0 && u && qdata && v, "apply_mass: bad arguments");
+    qf_apply_mass_kernel<<<grid_for(Q, 256), 256, 0, as_stream(stream)>>>(Q, u, qdata, v);
+    FEM_LAUNCH_CHECK();
+  });
+}
+
+int fem_b200_qfunction_build_mass(int dim, int64_t Q, const double* J, const double* w, double* qdata, void* stream) {
+  return guarded([&] {
+    require(dim >= 1 && dim <= 3, "build_mass: dim must be 1, 2 or 3");
+    require(Q > 0 && J && w && qdata, "build_mass: bad arguments");
+    qf_build_mass_kernel<<<grid_for(Q, 256), 256, 0, as_stream(stream)>>>(dim, Q, J, w, qdata);
+    FEM_LAUNCH_CHECK();
   });
 }
 
@@ -884,6 +1096,56 @@ int fem_b200_mass_apply_host(fem_b200_mass op, const double* u_host, int64_t n_u
     FEM_CUDA_CHECK(cudaMemcpyAsync(v_host, p.hv.get(), bytes, cudaMemcpyDeviceToHost, s));
     FEM_CUDA_CHECK(cudaStreamSynchronize(s));
     check_status(p);
+  });
+}
+
+int fem_b200_mass_autotune(fem_b200_mass op, const double* u, int64_t n_u, double* v, int64_t n_v, int reps,
+                           int* chosen, float* best_ms, void* stream) {
+  return guarded([&] {
+    require(op && op->d, "operator autotune: NULL handle");
+    MassPlan& p = *op->d;
+    require(n_u == p.l_size && u, "operator autotune: u must have l_size entries");
+    require(n_v == p.l_size && v, "operator autotune: v must have l_size entries");
+    require(reps >= 1 && reps <= 1000, "operator autotune: reps must be in 1..1000");
+    DeviceGuard g(p.device);
+    cudaStream_t s = as_stream(stream);
+    cudaEvent_t t0, t1;
+    FEM_CUDA_CHECK(cudaEventCreate(&t0));
+    FEM_CUDA_CHECK(cudaEventCreate(&t1));
+    int best = FEM_B200_KERNEL_SIMPLE;
+    float best_t = -1.0f;
+    try {
+      for (int variant = FEM_B200_KERNEL_SIMPLE; variant <= FEM_B200_KERNEL_OCCUPANCY; ++variant) {
+        ApplyLauncher l = variant_launcher(p, variant);
+        if (!l) continue;
+        p.launch = l;
+        for (int i = 0; i < 2; ++i) mass_apply_impl(p, u, v, false, s);  // warm-up (v is scratch)
+        FEM_CUDA_CHECK(cudaEventRecord(t0, s));
+        for (int i = 0; i < reps; ++i) mass_apply_impl(p, u, v, false, s);
+        FEM_CUDA_CHECK(cudaEventRecord(t1, s));
+        FEM_CUDA_CHECK(cudaEventSynchronize(t1));
+        check_status(p);
+        float ms = 0.0f;
+        FEM_CUDA_CHECK(cudaEventElapsedTime(&ms, t0, t1));
+        ms /= float(reps);
+        if (best_t < 0.0f || ms < best_t) best_t = ms, best = variant;
+      }
+    } catch (...) {
+      (void)cudaEventDestroy(t0);
+      (void)cudaEventDestroy(t1);
+      p.launch = variant_launcher(p, p.variant) ? variant_launcher(p, p.variant) : auto_kernel(p);
+      throw;
+    }
+    (void)cudaEventDestroy(t0);
+    (void)cudaEventDestroy(t1);
+    {
+      std::lock_guard<std::mutex> lock(g_tune_mu);
+      g_tune[tune_key(p)] = best;
+    }
+    p.variant = FEM_B200_KERNEL_AUTO;
+    p.launch = variant_launcher(p, best);
+    if (chosen) *chosen = best;
+    if (best_ms) *best_ms = best_t;
   });
 }
 

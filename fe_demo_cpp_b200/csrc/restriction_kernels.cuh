@@ -136,4 +136,29 @@ __global__ void weight_kernel(int dim, int Q, const double* __restrict__ w1, int
   }
 }
 
+// Pointwise mass QFunctions over Q points (include/qfunctions/mass.hpp):
+// v = qdata * u (component 0), and qdata = det(J) * w with J laid out
+// [d][c][p] and the reference's cofactor expansion.
+__global__ void qf_apply_mass_kernel(int64_t Q, const double* __restrict__ u, const double* __restrict__ qdata,
+                                     double* __restrict__ v) {
+  for (int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; p < Q; p += int64_t(gridDim.x) * blockDim.x)
+    v[p] = qdata[p] * u[p];
+}
+
+__global__ void qf_build_mass_kernel(int dim, int64_t Q, const double* __restrict__ J, const double* __restrict__ w,
+                                     double* __restrict__ qdata) {
+  for (int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; p < Q; p += int64_t(gridDim.x) * blockDim.x) {
+    auto j = [&](int d, int c) { return J[(int64_t(d) * dim + c) * Q + p]; };
+    double det;
+    if (dim == 1)
+      det = j(0, 0);
+    else if (dim == 2)
+      det = j(0, 0) * j(1, 1) - j(0, 1) * j(1, 0);
+    else
+      det = j(0, 0) * (j(1, 1) * j(2, 2) - j(1, 2) * j(2, 1)) - j(0, 1) * (j(1, 0) * j(2, 2) - j(1, 2) * j(2, 0)) +
+            j(0, 2) * (j(1, 0) * j(2, 1) - j(1, 1) * j(2, 0));
+    qdata[p] = det * w[p];
+  }
+}
+
 }  // namespace fem_b200

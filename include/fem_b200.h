@@ -57,7 +57,7 @@ extern "C" {
 #define FEM_B200_QF_APPLY_MASS 0        /* include/qfunctions/mass.hpp:45-51: component 0 only */
 #define FEM_B200_QF_APPLY_MASS_VECTOR 1 /* every component: v_k = qdata * u_k (no reference counterpart) */
 /* Kernel variants of the fused 3D mass apply (fem_b200_mass_set_kernel) */
-#define FEM_B200_KERNEL_AUTO 0      /* the fastest measured variant for the shape */
+#define FEM_B200_KERNEL_AUTO 0      /* the autotuned variant for the shape (fem_b200_mass_autotune), else SIMPLE */
 #define FEM_B200_KERNEL_SIMPLE 1    /* one CTA per 8-element tile, one element per thread */
 #define FEM_B200_KERNEL_PIPELINED 2 /* persistent CTAs, next tile staged by bulk copies during this one */
 #define FEM_B200_KERNEL_PAIRED 3    /* one CTA per 16 elements, two adjacent elements per thread */
@@ -158,6 +158,12 @@ int fem_b200_restriction_multiplicity(fem_b200_restriction r, double *mult, int6
 /* ========================================================================= */
 
 int fem_b200_basis_create(int dim, int num_comp, int P, int Q, int quad_mode, fem_b200_basis *out);
+
+/* A device basis from explicit 1D data (q_weight[Q], interp[Q*P], grad[Q*P]),
+ * e.g. the arrays of a TensorBasis the caller built or changed itself
+ * (include/basis.hpp:28-40 is a plain aggregate). */
+int fem_b200_basis_create_from(int dim, int num_comp, int P, int Q, const double *q_weight, const double *interp,
+                               const double *grad, fem_b200_basis *out);
 int fem_b200_basis_destroy(fem_b200_basis b);
 
 /* v (device) = basis action on u (device) for num_elem elements.  Interp and
@@ -187,6 +193,55 @@ int fem_b200_basis_apply(fem_b200_basis b, int num_elem, int t_mode, int eval_mo
  * overwrites the scratch it uses, so nothing needs clearing between calls. */
 int fem_b200_basis_apply_static(fem_b200_basis b, int num_elem, int t_mode, int eval_mode, const double *u,
                                 int64_t n_u, double *v, int64_t n_v, void *stream);
+
+/* ========================================================================= */
+/* Device memory and raw launchers                                            */
+/* (caller-owned device arrays; used by the C++ drop-in's DeviceArray and     */
+/* fem::cuda restriction, which own their index arrays like the reference's)  */
+/* ========================================================================= */
+
+/* cudaMalloc / cudaFree / copies (kind 0 H2D, 1 D2H, 2 D2D; H2D and D2H
+ * synchronise `stream`) / zero fill / stream synchronise.
+ * Replace the CUDA calls of fem::cuda::DeviceArray, include/cuda/device-array.hpp:18-95. */
+int fem_b200_malloc(void **ptr, size_t bytes);
+int fem_b200_free(void *ptr);
+int fem_b200_memcpy(void *dst, const void *src, size_t bytes, int kind, void *stream);
+int fem_b200_memset_zero(void *ptr, size_t bytes, void *stream);
+int fem_b200_synchronize(void *stream);
+
+/* Device limits: name (NUL-terminated, name_len bytes), ints[6] = {cc_major,
+ * cc_minor, sm_count, warp_size, max_threads_per_block, regs_per_block},
+ * sizes[5] = {shared_mem_per_block, ..._optin, shared_mem_per_sm,
+ * total_global_mem, free_global_mem}.
+ * Replaces fem::cuda::device_info, src/cuda/device-info.cpp:28-56. */
+int fem_b200_device_info(int device, char *name, int name_len, int *ints, int64_t *sizes);
+
+/* Restriction kernels on caller-owned device arrays (offsets [num_elem][elem_size]):
+ * gather (e_out overwritten), atomic scatter-add, transpose-map (deterministic)
+ * scatter-add, strided gather (t_mode 0) / scatter-add (t_mode 1) with host strides[3].
+ * Replace the five kernels of src/cuda/cuda-elem-restriction.cu:37-127. */
+int fem_b200_offset_gather(int num_elem, int elem_size, int num_comp, int comp_stride, const int *offsets,
+                           const double *l_in, double *e_out, void *stream);
+int fem_b200_offset_scatter_add(int num_elem, int elem_size, int num_comp, int comp_stride, const int *offsets,
+                                const double *e_in, double *l_out, void *stream);
+int fem_b200_transpose_scatter_add(int num_nodes, int num_elem, int elem_size, int num_comp, int comp_stride,
+                                   const int *l_vec_indices, const int *t_offsets, const int *t_indices,
+                                   const double *e_in, double *l_out, void *stream);
+int fem_b200_strided_apply(int t_mode, int num_elem, int elem_size, int num_comp, const int *strides,
+                           const double *in, double *out, void *stream);
+
+/* v (+)= t(j,b) u over one tensor mode, device arrays (t is J x B row-major,
+ * read transposed for t_mode = TRANSPOSE).
+ * Replaces fem::tensor_contract_apply, src/tensor-contract.cpp:35-59. */
+int fem_b200_contract(int64_t A, int B, int64_t C, int J, const double *t, int t_mode, int add, const double *u,
+                      double *v, void *stream);
+
+/* The two mass QFunctions pointwise over Q points (device arrays, [size][Q]):
+ * v = qdata * u, and qdata = det(J) * w with J [dim][dim][Q].
+ * Replace apply_mass / build_mass, include/qfunctions/mass.hpp:17-51, when
+ * run through qfunction_apply. */
+int fem_b200_qfunction_apply_mass(int64_t Q, const double *u, const double *qdata, double *v, void *stream);
+int fem_b200_qfunction_build_mass(int dim, int64_t Q, const double *J, const double *w, double *qdata, void *stream);
 
 /* ========================================================================= */
 /* Mass operator                                                              */
@@ -234,6 +289,16 @@ int fem_b200_mass_info(fem_b200_mass op, int *launches_per_apply, int *tile_elem
  * are dim-3 kernels; each is FEM_B200_ERROR_UNSUPPORTED where its shared
  * memory or thread count does not fit a CTA. */
 int fem_b200_mass_set_kernel(fem_b200_mass op, int variant);
+
+/* Autotuner: run every fused kernel variant the plan supports `reps` times
+ * on (u, v) -- device arrays of l_size; v is overwritten as scratch -- keep
+ * the fastest for this plan (CUDA-event timing on `stream`) and remember it
+ * for later plans with the same device, dim, P, Q, components, scatter mode
+ * and log2(num_elem) (FEM_B200_KERNEL_AUTO then starts from it).  *chosen
+ * receives the variant, *best_ms its time per apply (either may be NULL).
+ * Synchronises the stream. */
+int fem_b200_mass_autotune(fem_b200_mass op, const double *u, int64_t n_u, double *v, int64_t n_v, int reps,
+                           int *chosen, float *best_ms, void *stream);
 
 /* Synchronise `stream` and report a device-side failure of the plan's kernels
  * (a bounded wait that ran out) as FEM_B200_ERROR_CUDA.  fem_b200_mass_apply_host

@@ -215,6 +215,26 @@ def test_pipelined_equals_simple_on_many_tiles(fem, cuda, P, Q):
     assert np.array_equal(out[1], out[5])
 
 
+def test_autotune_picks_a_variant_and_keeps_parity(fem, cuda, orc):
+    import torch
+    m = box_mesh((12, 10, 9), 5, seed=3)
+    qd = build_qdata(fem, cuda, m, 6)
+    op = fem.MassOperator(fem.Restriction(m.num_elem, 125, 1, m.num_nodes, m.num_nodes, m.offsets),
+                          fem.Basis(3, 1, 5, 6), qd)
+    u = dev(random_vector(m.num_nodes, 1), cuda)
+    scratch = torch.empty_like(u)
+    name, ms = op.autotune(u, scratch, reps=3)
+    assert name in ("simple", "pipelined", "paired", "prefetch", "occupancy") and ms > 0
+    assert op.info()["kernel"] == name
+    v = torch.empty_like(u)
+    op.apply(u, v)
+    close(host(v), orc.mass_apply(3, m.num_elem, 5, 6, 1, m.num_nodes, m.num_nodes, m.offsets, host(qd), host(u)))
+    # a new plan of the same shape starts from the tuned choice
+    op2 = fem.MassOperator(fem.Restriction(m.num_elem, 125, 1, m.num_nodes, m.num_nodes, m.offsets),
+                           fem.Basis(3, 1, 5, 6), qd)
+    assert op2.info()["kernel"] == name
+
+
 def test_pipelined_unavailable_where_smem_does_not_fit(fem, cuda):
     import torch
     m = box_mesh((1, 1, 1), 8, seed=0)
