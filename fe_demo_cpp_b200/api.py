@@ -296,6 +296,22 @@ class MassOperator(_Handle):
              C.addressof(ms), _stream(stream))
         return KernelVariant(chosen.value).name, ms.value
 
+    def diagonal(self, diag, stream=None) -> None:
+        """diag (device, l_size) = the assembled diagonal of M."""
+        _check_dev(diag)
+        call("fem_b200_mass_diagonal", self.h, _ptr(diag), _n(diag), _stream(stream))
+
+    def solve(self, f, u, rtol=1e-10, max_iter=1000, precision="fp64", stream=None) -> dict:
+        """Solve M u = f (device arrays) by Jacobi PCG; precision 'fp64' or
+        'fp32_ir' (FP32 inner PCG in FP64 iterative refinement)."""
+        _check_dev(f)
+        _check_dev(u)
+        prec = {"fp64": 0, "fp32_ir": 1}[precision]
+        its, outer, rel = C.c_int(0), C.c_int(0), C.c_double(0.0)
+        call("fem_b200_mass_solve", self.h, _ptr(f), _n(f), _ptr(u), _n(u), float(rtol), int(max_iter), prec,
+             C.addressof(its), C.addressof(outer), C.addressof(rel), _stream(stream))
+        return {"iterations": its.value, "refinements": outer.value, "rel_residual": rel.value}
+
     def check(self, stream=None) -> None:
         """Synchronise and raise if a device-side wait of the plan's kernels ran out."""
         call("fem_b200_mass_check", self.h, _stream(stream))

@@ -26,11 +26,11 @@
 
 namespace fem_b200 {
 
-template <int P, int Q>
+template <int P, int Q, class T = double>
 struct Mat1D {
-  double B[Q * P];  // interp_1d, row-major [q][p]
-  double G[Q * P];  // grad_1d
-  double W[Q];      // q_weight_1d
+  T B[Q * P];  // interp_1d, row-major [q][p]
+  T G[Q * P];  // grad_1d (the diagonal kernels carry interp_1d squared here)
+  T W[Q];      // q_weight_1d
 };
 
 // Shared-memory plane stride for a tile of 8 elements: an odd multiple of 8
@@ -47,7 +47,7 @@ __host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
 //   qdata    [tile][qx][col][e]     col = q / Q  (the other axes), q = qx + Q*col
 // Elements past num_elem are padding (offset 0, qdata 0) and never scattered.
 // ---------------------------------------------------------------------------
-__global__ void tile_offsets_kernel(const int* __restrict__ offsets, int num_elem, int elem_size, int E,
+static __global__ void tile_offsets_kernel(const int* __restrict__ offsets, int num_elem, int elem_size, int E,
                                     int64_t n_out, int* __restrict__ out) {
   for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < n_out; t += int64_t(gridDim.x) * blockDim.x) {
     const int64_t el = t % E, rest = t / E;
@@ -57,7 +57,7 @@ __global__ void tile_offsets_kernel(const int* __restrict__ offsets, int num_ele
   }
 }
 
-__global__ void tile_qdata_kernel(const double* __restrict__ qdata, int num_elem, int Q, int nq, int E, int64_t n_out,
+static __global__ void tile_qdata_kernel(const double* __restrict__ qdata, int num_elem, int Q, int nq, int E, int64_t n_out,
                                   double* __restrict__ out) {
   const int ncol = nq / Q;
   for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < n_out; t += int64_t(gridDim.x) * blockDim.x) {
@@ -106,16 +106,16 @@ struct Mass3D {
 // mode; a transpose-map reduction follows).
 // MINB > 1 asks for MINB resident CTAs per SM (a register cap), trading a
 // little spilling for more warps to hide memory latency.
-template <int P, int Q, int MINB = 1>
+template <int P, int Q, int MINB = 1, class T = double>
 __global__ void __launch_bounds__(Mass3D<P, Q>::NT, MINB) mass3d_apply_kernel(
-    const __grid_constant__ Mat1D<P, Q> m, const int* __restrict__ offs, const double* __restrict__ qd,
-    const double* __restrict__ u, double* __restrict__ v, double* __restrict__ ev, int num_elem, int num_comp_run,
+    const __grid_constant__ Mat1D<P, Q, T> m, const int* __restrict__ offs, const T* __restrict__ qd,
+    const T* __restrict__ u, T* __restrict__ v, T* __restrict__ ev, int num_elem, int num_comp_run,
     int64_t comp_stride) {
   using L = Mass3D<P, Q>;
   constexpr int E = L::E;
-  extern __shared__ double smem[];
-  double* sa = smem;
-  double* sb = smem + L::SA;
+  extern __shared__ __align__(16) unsigned char smem_bytes[];
+  T* sa = reinterpret_cast<T*>(smem_bytes);
+  T* sb = sa + L::SA;
   const int t = threadIdx.x, e = t % E, col = t / E;
   const int64_t tile = blockIdx.x;
   const int64_t eg = tile * E + e;
@@ -124,9 +124,9 @@ __global__ void __launch_bounds__(Mass3D<P, Q>::NT, MINB) mass3d_apply_kernel(
   const bool mixed = col < P * Q;  // (px, qz) = (col % P, col / P)
 
   // Prefetch: this thread's qdata row (qy, qz) = (col % Q, col / Q), all qx.
-  double qv[Q];
+  T qv[Q];
   {
-    const double* qt = qd + tile * (int64_t(L::NQ) * E) + col * E + e;
+    const T* qt = qd + tile * (int64_t(L::NQ) * E) + col * E + e;
 #pragma unroll
     for (int qx = 0; qx < Q; ++qx) qv[qx] = __ldg(qt + qx * (Q * Q * E));
   }
@@ -140,13 +140,13 @@ __global__ void __launch_bounds__(Mass3D<P, Q>::NT, MINB) mass3d_apply_kernel(
   for (int k = 0; k < num_comp_run; ++k) {
     const int64_t ks = k * comp_stride;
     if (nodal) {  // phase A
-      double x[P];
+      T x[P];
 #pragma unroll
       for (int pz = 0; pz < P; ++pz) x[pz] = __ldg(u + off[pz] + ks);
       const int px = col % P, py = col / P;
 #pragma unroll
       for (int qz = 0; qz < Q; ++qz) {
-        double s = 0.0;
+        T s = T(0);
 #pragma unroll
         for (int pz = 0; pz < P; ++pz) s += m.B[qz * P + pz] * x[pz];
         sa[py * L::PS1 + (qz * P + px) * E + e] = s;
@@ -154,13 +154,13 @@ __global__ void __launch_bounds__(Mass3D<P, Q>::NT, MINB) mass3d_apply_kernel(
     }
     __syncthreads();
     if (mixed) {  // phase B
-      double y[P];
+      T y[P];
 #pragma unroll
       for (int py = 0; py < P; ++py) y[py] = sa[py * L::PS1 + col * E + e];
       const int px = col % P, qz = col / P;
 #pragma unroll
       for (int qy = 0; qy < Q; ++qy) {
-        double s = 0.0;
+        T s = T(0);
 #pragma unroll
         for (int py = 0; py < P; ++py) s += m.B[qy * P + py] * y[py];
         sb[px * L::PS2 + (qz * Q + qy) * E + e] = s;
@@ -168,13 +168,13 @@ __global__ void __launch_bounds__(Mass3D<P, Q>::NT, MINB) mass3d_apply_kernel(
     }
     __syncthreads();
     {  // phase C: x, pointwise mass, x^T
-      double w[P];
+      T w[P];
 #pragma unroll
       for (int px = 0; px < P; ++px) w[px] = sb[px * L::PS2 + col * E + e];
-      double r[Q];
+      T r[Q];
 #pragma unroll
       for (int qx = 0; qx < Q; ++qx) {
-        double s = 0.0;
+        T s = T(0);
 #pragma unroll
         for (int px = 0; px < P; ++px) s += m.B[qx * P + px] * w[px];
         r[qx] = qv[qx] * s;
@@ -182,7 +182,7 @@ __global__ void __launch_bounds__(Mass3D<P, Q>::NT, MINB) mass3d_apply_kernel(
       const int qy = col % Q, qz = col / Q;
 #pragma unroll
       for (int px = 0; px < P; ++px) {
-        double s = 0.0;
+        T s = T(0);
 #pragma unroll
         for (int qx = 0; qx < Q; ++qx) s += m.B[qx * P + px] * r[qx];
         sa[qy * L::PS3 + (qz * P + px) * E + e] = s;
@@ -190,13 +190,13 @@ __global__ void __launch_bounds__(Mass3D<P, Q>::NT, MINB) mass3d_apply_kernel(
     }
     __syncthreads();
     if (mixed) {  // phase F: y^T
-      double y[Q];
+      T y[Q];
 #pragma unroll
       for (int qy = 0; qy < Q; ++qy) y[qy] = sa[qy * L::PS3 + col * E + e];
       const int px = col % P, qz = col / P;
 #pragma unroll
       for (int py = 0; py < P; ++py) {
-        double s = 0.0;
+        T s = T(0);
 #pragma unroll
         for (int qy = 0; qy < Q; ++qy) s += m.B[qy * P + py] * y[qy];
         sb[qz * L::PS4 + (py * P + px) * E + e] = s;
@@ -204,12 +204,12 @@ __global__ void __launch_bounds__(Mass3D<P, Q>::NT, MINB) mass3d_apply_kernel(
     }
     __syncthreads();
     if (nodal) {  // phase G: z^T and the scatter
-      double z[Q];
+      T z[Q];
 #pragma unroll
       for (int qz = 0; qz < Q; ++qz) z[qz] = sb[qz * L::PS4 + col * E + e];
 #pragma unroll
       for (int pz = 0; pz < P; ++pz) {
-        double s = 0.0;
+        T s = T(0);
 #pragma unroll
         for (int qz = 0; qz < Q; ++qz) s += m.B[qz * P + pz] * z[qz];
         if (valid) {
@@ -359,24 +359,24 @@ struct Mass2D {
   static constexpr int ES = P * P, NQ = Q * Q;
 };
 
-template <int P, int Q>
+template <int P, int Q, class T = double>
 __global__ void __launch_bounds__(Mass2D<P, Q>::NT) mass2d_apply_kernel(
-    const __grid_constant__ Mat1D<P, Q> m, const int* __restrict__ offs, const double* __restrict__ qd,
-    const double* __restrict__ u, double* __restrict__ v, double* __restrict__ ev, int num_elem, int num_comp_run,
+    const __grid_constant__ Mat1D<P, Q, T> m, const int* __restrict__ offs, const T* __restrict__ qd,
+    const T* __restrict__ u, T* __restrict__ v, T* __restrict__ ev, int num_elem, int num_comp_run,
     int64_t comp_stride) {
   using L = Mass2D<P, Q>;
   constexpr int E = L::E;
-  extern __shared__ double smem[];
-  double* s1 = smem;
-  double* s3 = smem + L::S1;
+  extern __shared__ __align__(16) unsigned char smem_bytes[];
+  T* s1 = reinterpret_cast<T*>(smem_bytes);
+  T* s3 = s1 + L::S1;
   const int t = threadIdx.x, e = t % E, col = t / E;
   const int64_t tile = blockIdx.x;
   const int64_t eg = tile * E + e;
   const bool valid = eg < num_elem;
   const bool nodal = col < P;
-  double qv[Q];
+  T qv[Q];
   {
-    const double* qt = qd + tile * (int64_t(L::NQ) * E) + col * E + e;
+    const T* qt = qd + tile * (int64_t(L::NQ) * E) + col * E + e;
 #pragma unroll
     for (int qx = 0; qx < Q; ++qx) qv[qx] = __ldg(qt + qx * (Q * E));
   }
@@ -389,12 +389,12 @@ __global__ void __launch_bounds__(Mass2D<P, Q>::NT) mass2d_apply_kernel(
   for (int k = 0; k < num_comp_run; ++k) {
     const int64_t ks = k * comp_stride;
     if (nodal) {
-      double x[P];
+      T x[P];
 #pragma unroll
       for (int py = 0; py < P; ++py) x[py] = __ldg(u + off[py] + ks);
 #pragma unroll
       for (int qy = 0; qy < Q; ++qy) {
-        double s = 0.0;
+        T s = T(0);
 #pragma unroll
         for (int py = 0; py < P; ++py) s += m.B[qy * P + py] * x[py];
         s1[(col * Q + qy) * E + e] = s;
@@ -402,20 +402,20 @@ __global__ void __launch_bounds__(Mass2D<P, Q>::NT) mass2d_apply_kernel(
     }
     __syncthreads();
     {
-      double w[P];
+      T w[P];
 #pragma unroll
       for (int px = 0; px < P; ++px) w[px] = s1[(px * Q + col) * E + e];
-      double r[Q];
+      T r[Q];
 #pragma unroll
       for (int qx = 0; qx < Q; ++qx) {
-        double s = 0.0;
+        T s = T(0);
 #pragma unroll
         for (int px = 0; px < P; ++px) s += m.B[qx * P + px] * w[px];
         r[qx] = qv[qx] * s;
       }
 #pragma unroll
       for (int px = 0; px < P; ++px) {
-        double s = 0.0;
+        T s = T(0);
 #pragma unroll
         for (int qx = 0; qx < Q; ++qx) s += m.B[qx * P + px] * r[qx];
         s3[(col * P + px) * E + e] = s;
@@ -423,12 +423,12 @@ __global__ void __launch_bounds__(Mass2D<P, Q>::NT) mass2d_apply_kernel(
     }
     __syncthreads();
     if (nodal) {
-      double z[Q];
+      T z[Q];
 #pragma unroll
       for (int qy = 0; qy < Q; ++qy) z[qy] = s3[(qy * P + col) * E + e];
 #pragma unroll
       for (int py = 0; py < P; ++py) {
-        double s = 0.0;
+        T s = T(0);
 #pragma unroll
         for (int qy = 0; qy < Q; ++qy) s += m.B[qy * P + py] * z[qy];
         if (valid) {
@@ -508,37 +508,37 @@ __global__ void __launch_bounds__(32 * Q) mass2d_build_kernel(const __grid_const
 // ---------------------------------------------------------------------------
 // dim = 1: one thread per element, everything in registers.
 // ---------------------------------------------------------------------------
-template <int P, int Q>
-__global__ void __launch_bounds__(128) mass1d_apply_kernel(const __grid_constant__ Mat1D<P, Q> m,
-                                                          const int* __restrict__ offs, const double* __restrict__ qd,
-                                                          const double* __restrict__ u, double* __restrict__ v,
-                                                          double* __restrict__ ev, int num_elem, int num_comp_run,
+template <int P, int Q, class T = double>
+__global__ void __launch_bounds__(128) mass1d_apply_kernel(const __grid_constant__ Mat1D<P, Q, T> m,
+                                                          const int* __restrict__ offs, const T* __restrict__ qd,
+                                                          const T* __restrict__ u, T* __restrict__ v,
+                                                          T* __restrict__ ev, int num_elem, int num_comp_run,
                                                           int64_t comp_stride) {
   constexpr int E = 128;
   const int e = threadIdx.x;
   const int64_t tile = blockIdx.x, eg = tile * E + e;
   if (eg >= num_elem) return;
   int off[P];
-  double qv[Q];
+  T qv[Q];
 #pragma unroll
   for (int px = 0; px < P; ++px) off[px] = __ldg(offs + (tile * P + px) * E + e);
 #pragma unroll
   for (int qx = 0; qx < Q; ++qx) qv[qx] = __ldg(qd + (tile * Q + qx) * E + e);
   for (int k = 0; k < num_comp_run; ++k) {
     const int64_t ks = k * comp_stride;
-    double x[P], r[Q];
+    T x[P], r[Q];
 #pragma unroll
     for (int px = 0; px < P; ++px) x[px] = __ldg(u + off[px] + ks);
 #pragma unroll
     for (int qx = 0; qx < Q; ++qx) {
-      double s = 0.0;
+      T s = T(0);
 #pragma unroll
       for (int px = 0; px < P; ++px) s += m.B[qx * P + px] * x[px];
       r[qx] = qv[qx] * s;
     }
 #pragma unroll
     for (int px = 0; px < P; ++px) {
-      double s = 0.0;
+      T s = T(0);
 #pragma unroll
       for (int qx = 0; qx < Q; ++qx) s += m.B[qx * P + px] * r[qx];
       if (ev)

@@ -1,0 +1,190 @@
+// Shared host-side types of libfem_b200: device buffers, restriction /
+// basis / mass-plan state, launch helpers.  Used by device.cu (the operator
+// entry points) and solver.cu (diagonal, mixed-precision solves).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "common.hpp"
+#include "fem_b200.h"
+#include "host_setup.hpp"
+#include "mass_kernels.cuh"
+
+namespace fem_b200 {
+
+// ---------------------------------------------------------------------------
+// RAII device buffer (move-only), the reference's DeviceArray semantics
+// (include/cuda/device-array.hpp:18-95) without the synchronous copies.
+// ---------------------------------------------------------------------------
+template <class T>
+class DevBuf {
+ public:
+  DevBuf() = default;
+  explicit DevBuf(size_t n) { alloc(n); }
+  ~DevBuf() { release(); }
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : p_(o.p_), n_(o.n_) { o.p_ = nullptr, o.n_ = 0; }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    if (this != &o) {
+      release();
+      p_ = o.p_, n_ = o.n_;
+      o.p_ = nullptr, o.n_ = 0;
+    }
+    return *this;
+  }
+  void alloc(size_t n) {
+    release();
+    if (n == 0) return;
+    FEM_CUDA_CHECK(cudaMalloc(&p_, n * sizeof(T)));
+    n_ = n;
+  }
+  T* get() const { return p_; }
+  size_t size() const { return n_; }
+  size_t bytes() const { return n_ * sizeof(T); }
+
+ private:
+  void release() noexcept {
+    if (p_) (void)cudaFree(p_);
+    p_ = nullptr, n_ = 0;
+  }
+  T* p_ = nullptr;
+  size_t n_ = 0;
+};
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    FEM_CUDA_CHECK(cudaGetDevice(&prev));
+    if (prev != dev) FEM_CUDA_CHECK(cudaSetDevice(dev));
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    if (cudaGetDevice(&cur) == cudaSuccess && cur != prev && prev >= 0) (void)cudaSetDevice(prev);
+  }
+};
+
+inline int current_device() {
+  int d = 0;
+  FEM_CUDA_CHECK(cudaGetDevice(&d));
+  return d;
+}
+
+inline cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
+
+inline int grid_for(int64_t n, int threads) {
+  const int64_t b = (n + threads - 1) / threads;
+  return int(std::max<int64_t>(1, std::min<int64_t>(b, 148LL * 64)));
+}
+
+#define FEM_LAUNCH_CHECK() FEM_CUDA_CHECK(cudaGetLastError())
+
+// ---------------------------------------------------------------------------
+// Restriction
+// ---------------------------------------------------------------------------
+struct RestrictionData {
+  int device = 0;
+  bool strided = false;
+  int num_elem = 0, elem_size = 0, num_comp = 0, comp_stride = 0, l_size = 0;
+  int64_t e_size = 0;
+  int64_t strides[3] = {0, 0, 0};
+  int scatter_mode = FEM_B200_SCATTER_ATOMIC;
+  DevBuf<int> offsets;  // [num_elem][elem_size]
+  int num_nodes = 0;    // transpose map (deterministic offset restrictions)
+  DevBuf<int> l_vec_indices, t_offsets, t_indices;
+};
+
+// ---------------------------------------------------------------------------
+// Basis: host data plus device copies for the generic contraction kernels
+// ---------------------------------------------------------------------------
+struct BasisDev {
+  int device = 0;
+  BasisData h;
+  DevBuf<double> interp, grad, weight;
+  DevBuf<double> scratch;  // ping-pong pass buffers, grown on demand
+  std::mutex scratch_mu;
+};
+
+// ---------------------------------------------------------------------------
+// Mass plan
+// ---------------------------------------------------------------------------
+struct MassPlan;
+using ApplyLauncher = void (*)(const MassPlan&, const double*, double*, double*, cudaStream_t);
+using BuildLauncher = void (*)(const BasisData&, const RestrictionData&, const double*, double*, cudaStream_t);
+
+struct MassPlan {
+  int device = 0;
+  int dim = 0, P = 0, Q = 0, num_comp = 0, comp_run = 0, qf = 0, scatter_mode = 0;
+  int num_elem = 0, l_size = 0, es = 0, nq = 0;
+  int64_t comp_stride = 0;
+  int tile_e = 0;
+  int64_t n_tiles = 0;
+  BasisData basis;
+  std::shared_ptr<RestrictionData> r;
+  DevBuf<int> offs_t;
+  DevBuf<double> qd_t;
+  DevBuf<double> evec;    // deterministic mode: element contributions
+  DevBuf<double> hu, hv;  // staging for the host-memory apply
+  DevBuf<int> status;     // device status word (bit 0: a bounded wait ran out)
+  ApplyLauncher launch = nullptr;       // the kernel in use
+  ApplyLauncher launch_simple = nullptr;
+  ApplyLauncher launch_pipe = nullptr;  // nullptr where the pipelined kernel does not apply
+  ApplyLauncher launch_x2 = nullptr;    // two elements per thread (dim 3)
+  ApplyLauncher launch_pf = nullptr;    // persistent, prefetching (dim 3)
+  ApplyLauncher launch_occ = nullptr;   // one-tile CTAs, register-capped for occupancy (dim 3)
+  int variant = FEM_B200_KERNEL_AUTO;
+  // solver state (solver.cu), allocated by the first solve
+  DevBuf<double> diag, dinv;                      // assembled diagonal and its inverse
+  DevBuf<double> cg_r, cg_z, cg_p, cg_ap;         // FP64 CG vectors / outer residual
+  DevBuf<double> red;                             // device scalars of the reductions
+  DevBuf<float> qd_t32, dinv32;                   // FP32 copies for the inner solves
+  DevBuf<float> f_r, f_z, f_p, f_ap, f_x;         // FP32 CG vectors
+};
+
+template <int P, int Q>
+Mat1D<P, Q> make_mat(const BasisData& b) {
+  Mat1D<P, Q> m;
+  std::memcpy(m.B, b.interp.data(), sizeof(m.B));
+  std::memcpy(m.G, b.grad.data(), sizeof(m.G));
+  std::memcpy(m.W, b.q_weight.data(), sizeof(m.W));
+  return m;
+}
+
+constexpr int kMaxSmemPerCta = 227 * 1024;
+
+// Opt a kernel into more than 48 KB of dynamic shared memory, once per device
+// (the attribute belongs to the device context).
+template <class K>
+void set_smem(K kernel, int bytes, std::atomic<uint64_t>& done) {
+  if (bytes <= 48 * 1024) return;
+  const int dev = current_device();
+  const uint64_t bit = uint64_t(1) << (dev & 63);
+  if (done.load() & bit) return;
+  FEM_CUDA_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  done.fetch_or(bit);
+}
+
+// Defined in device.cu.
+void check_status(MassPlan& p);
+void mass_apply_impl(MassPlan& p, const double* u, double* v, bool zero, cudaStream_t s);
+std::string shape_str(int dim, int P, int Q);
+
+}  // namespace fem_b200
+
+// The C ABI's opaque handles.
+struct fem_b200_restriction_s {
+  std::shared_ptr<fem_b200::RestrictionData> d;
+};
+struct fem_b200_basis_s {
+  std::unique_ptr<fem_b200::BasisDev> d;
+};
+struct fem_b200_mass_s {
+  std::unique_ptr<fem_b200::MassPlan> d;
+};

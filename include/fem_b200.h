@@ -300,6 +300,32 @@ int fem_b200_mass_set_kernel(fem_b200_mass op, int variant);
 int fem_b200_mass_autotune(fem_b200_mass op, const double *u, int64_t n_u, double *v, int64_t n_v, int reps,
                            int *chosen, float *best_ms, void *stream);
 
+/* Assembled diagonal of the mass operator, diag (device, l_size), overwritten:
+ * diag_i = sum over elements and quadrature points of qdata * (phi_i)^2, one
+ * fused kernel (interp^T with the squared 1D matrix applied to qdata, then
+ * the scatter-add); every component of a vector plan gets the same diagonal.
+ * The Jacobi preconditioner of fem_b200_mass_solve.  No reference counterpart
+ * (its survey verifies it against e_i^T M e_i on small meshes). */
+int fem_b200_mass_diagonal(fem_b200_mass op, double *diag, int64_t n, void *stream);
+
+/* Solve M u = f (device arrays, l_size) by Jacobi-preconditioned CG from u = 0.
+ *   FEM_B200_SOLVE_FP64     FP64 PCG to ||r|| <= rtol ||f|| (recursive residual);
+ *   FEM_B200_SOLVE_FP32_IR  FP64 iterative refinement: r = f - M u in FP64, a
+ *                           correction from FP32 PCG (FP32 qdata, vectors and
+ *                           fused apply; FP64 dot products) on r / ||r|| to 1e-5,
+ *                           until ||f - M u|| <= rtol ||f||.
+ * max_iter bounds the CG iterations (all inner ones for FP32_IR).  Outputs (any
+ * may be NULL): total CG iterations, refinement steps, and the true FP64
+ * relative residual ||f - M u|| / ||f|| (one extra FP64 apply).  Synchronises
+ * the stream.  Plans of the reference apply_mass with num_comp > 1 are
+ * singular (components 1.. are left out) and return FEM_B200_ERROR_UNSUPPORTED.
+ * No reference counterpart (the reference has no solver). */
+#define FEM_B200_SOLVE_FP64 0
+#define FEM_B200_SOLVE_FP32_IR 1
+int fem_b200_mass_solve(fem_b200_mass op, const double *f, int64_t n_f, double *u, int64_t n_u, double rtol,
+                        int max_iter, int precision, int *iterations, int *refinements, double *rel_residual,
+                        void *stream);
+
 /* Synchronise `stream` and report a device-side failure of the plan's kernels
  * (a bounded wait that ran out) as FEM_B200_ERROR_CUDA.  fem_b200_mass_apply_host
  * does this check itself. */
