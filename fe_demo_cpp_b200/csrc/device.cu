@@ -34,7 +34,8 @@ void launch_apply3(const MassPlan& p, const double* u, double* v, double* ev, cu
   static std::atomic<uint64_t> smem_set{0};
   set_smem(mass3d_apply_kernel<P, Q, MINB>, L::SMEM, smem_set);
   mass3d_apply_kernel<P, Q, MINB><<<unsigned(p.n_tiles), L::NT, L::SMEM, s>>>(
-      make_mat<P, Q>(p.basis), p.offs_t.get(), p.qd_t.get(), u, v, ev, p.num_elem, p.comp_run, p.comp_stride);
+      make_mat<P, Q>(p.basis), p.offs_t.get(), p.qd_t.get(), u, v, ev, p.num_elem, p.comp_run, p.comp_stride,
+      ApplyPlain{});
   FEM_LAUNCH_CHECK();
 }
 
@@ -42,23 +43,7 @@ void launch_apply3(const MassPlan& p, const double* u, double* v, double* ev, cu
 // most one CTA per tile.
 template <class K>
 int persistent_grid(K kernel, int threads, int smem, int64_t n_tiles) {
-  static std::mutex mu;
-  static int cached[64] = {};
-  const int dev = current_device();
-  int per_grid = 0;
-  {
-    std::lock_guard<std::mutex> lock(mu);
-    if (dev < 64 && cached[dev]) per_grid = cached[dev];
-  }
-  if (!per_grid) {
-    int sms = 0, blocks = 0;
-    FEM_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    FEM_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, threads, smem));
-    per_grid = sms * std::max(blocks, 1);
-    std::lock_guard<std::mutex> lock(mu);
-    if (dev < 64) cached[dev] = per_grid;
-  }
-  return int(std::min<int64_t>(n_tiles, per_grid));
+  return int(std::min<int64_t>(n_tiles, resident_ctas(reinterpret_cast<const void*>(kernel), threads, smem)));
 }
 
 template <int P, int Q>
@@ -103,7 +88,8 @@ void launch_apply2(const MassPlan& p, const double* u, double* v, double* ev, cu
   static std::atomic<uint64_t> smem_set{0};
   set_smem(mass2d_apply_kernel<P, Q>, L::SMEM, smem_set);
   mass2d_apply_kernel<P, Q><<<unsigned(p.n_tiles), L::NT, L::SMEM, s>>>(
-      make_mat<P, Q>(p.basis), p.offs_t.get(), p.qd_t.get(), u, v, ev, p.num_elem, p.comp_run, p.comp_stride);
+      make_mat<P, Q>(p.basis), p.offs_t.get(), p.qd_t.get(), u, v, ev, p.num_elem, p.comp_run, p.comp_stride,
+      ApplyPlain{});
   FEM_LAUNCH_CHECK();
 }
 
@@ -111,7 +97,7 @@ template <int P, int Q>
 void launch_apply1(const MassPlan& p, const double* u, double* v, double* ev, cudaStream_t s) {
   mass1d_apply_kernel<P, Q><<<unsigned(p.n_tiles), 128, 0, s>>>(make_mat<P, Q>(p.basis), p.offs_t.get(),
                                                                  p.qd_t.get(), u, v, ev, p.num_elem, p.comp_run,
-                                                                 p.comp_stride);
+                                                                 p.comp_stride, ApplyPlain{});
   FEM_LAUNCH_CHECK();
 }
 

@@ -7,9 +7,11 @@
 #include <algorithm>
 #include <atomic>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "common.hpp"
@@ -57,6 +59,27 @@ class DevBuf {
   }
   T* p_ = nullptr;
   size_t n_ = 0;
+};
+
+// RAII page-locked host buffer.
+template <class T>
+class PinnedBuf {
+ public:
+  PinnedBuf() = default;
+  ~PinnedBuf() {
+    if (p_) (void)cudaFreeHost(p_);
+  }
+  PinnedBuf(const PinnedBuf&) = delete;
+  PinnedBuf& operator=(const PinnedBuf&) = delete;
+  void alloc(size_t n) {
+    if (p_) (void)cudaFreeHost(p_);
+    p_ = nullptr;
+    FEM_CUDA_CHECK(cudaMallocHost(&p_, n * sizeof(T)));
+  }
+  T* get() const { return p_; }
+
+ private:
+  T* p_ = nullptr;
 };
 
 struct DeviceGuard {
@@ -141,11 +164,13 @@ struct MassPlan {
   ApplyLauncher launch_occ = nullptr;   // one-tile CTAs, register-capped for occupancy (dim 3)
   int variant = FEM_B200_KERNEL_AUTO;
   // solver state (solver.cu), allocated by the first solve
-  DevBuf<double> diag, dinv;                      // assembled diagonal and its inverse
-  DevBuf<double> cg_r, cg_z, cg_p, cg_ap;         // FP64 CG vectors / outer residual
-  DevBuf<double> red;                             // device scalars of the reductions
-  DevBuf<float> qd_t32, dinv32;                   // FP32 copies for the inner solves
-  DevBuf<float> f_r, f_z, f_p, f_ap, f_x;         // FP32 CG vectors
+  DevBuf<double> diag, dinv;              // assembled diagonal and its inverse
+  DevBuf<double> cg_r, cg_p, cg_s, cg_w;  // FP64 Krylov vectors (cg_r, cg_w: outer residual, M u)
+  DevBuf<double> part;                    // per-CTA partial sums of the grid reductions
+  DevBuf<CgScalars> cg_st;                // device-resident solver scalars
+  PinnedBuf<CgScalars> cg_host;           // their host copy
+  DevBuf<float> qd_t32, dinv32, evec32;   // FP32 copies for the inner solves
+  DevBuf<float> f_r, f_p, f_s, f_w, f_x;  // FP32 Krylov vectors
 };
 
 template <int P, int Q>
@@ -158,6 +183,33 @@ Mat1D<P, Q> make_mat(const BasisData& b) {
 }
 
 constexpr int kMaxSmemPerCta = 227 * 1024;
+
+// SMs x resident CTAs per SM of `kernel` on the current device (occupancy
+// calculator), cached per (kernel, device, threads, shared memory).
+inline int resident_ctas(const void* kernel, int threads, int smem) {
+  struct Key {
+    const void* k;
+    int dev, threads, smem;
+    bool operator<(const Key& o) const {
+      return std::tie(k, dev, threads, smem) < std::tie(o.k, o.dev, o.threads, o.smem);
+    }
+  };
+  static std::mutex mu;
+  static std::map<Key, int> cache;
+  const Key key{kernel, current_device(), threads, smem};
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+  }
+  int sms = 0, blocks = 0;
+  FEM_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, key.dev));
+  FEM_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, threads, smem));
+  const int g = sms * std::max(blocks, 1);
+  std::lock_guard<std::mutex> lock(mu);
+  cache[key] = g;
+  return g;
+}
 
 // Opt a kernel into more than 48 KB of dynamic shared memory, once per device
 // (the attribute belongs to the device context).

@@ -1,11 +1,14 @@
 // Jacobi-preconditioned CG mass solves on the device (sm_100a):
 //   * the assembled diagonal of the mass operator, one fused kernel;
-//   * the FP32 instantiation of the fused apply (inner solves);
+//   * Chronopoulos-Gear PCG (one reduction point per iteration) whose scalars
+//     stay on the device, so the host queues iterations without waiting;
+//     the Jacobi scaling is folded into the apply's gather and (u, M u) into
+//     its quadrature-point pass (apply_ext.cuh);
 //   * FP64 PCG, and FP32 PCG inside FP64 iterative refinement.
-// CG dot products accumulate in FP64 in every precision; the outer residual
-// of the refinement is an FP64 apply.  The reference has no solver; this is
-// the growth direction its survey names (Jacobi diagonal + CG + mixed-
-// precision refinement), tested against a host FP64 CG around the oracle.
+// Reductions accumulate in FP64 in every precision, in a fixed order; the
+// outer residual of the refinement is an FP64 apply.  The reference has no
+// solver: these solve M u = f with its mass operator and are tested against
+// the oracle's apply (f = M u* for a known u*).
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -26,8 +29,8 @@ template <int P, int Q>
 __global__ void __launch_bounds__(Mass3D<P, Q>::NT) mass3d_diag_kernel(const __grid_constant__ Mat1D<P, Q> m,
                                                                       const int* __restrict__ offs,
                                                                       const double* __restrict__ qd,
-                                                                      double* __restrict__ diag, int num_elem,
-                                                                      int num_comp, int64_t comp_stride) {
+                                                                      double* __restrict__ diag, double* __restrict__ ev,
+                                                                      int num_elem, int num_comp, int64_t comp_stride) {
   using L = Mass3D<P, Q>;
   constexpr int E = L::E;
   extern __shared__ __align__(16) unsigned char smem_bytes[];
@@ -76,7 +79,12 @@ __global__ void __launch_bounds__(Mass3D<P, Q>::NT) mass3d_diag_kernel(const __g
 #pragma unroll
       for (int qz = 0; qz < Q; ++qz) s += m.B[qz * P + pz] * z[qz];
       const int64_t off = ot[pz * (P * P * E)];
-      for (int k = 0; k < num_comp; ++k) atomicAdd(diag + off + k * comp_stride, s);
+      for (int k = 0; k < num_comp; ++k) {
+        if (ev)
+          ev[(int64_t(k) * L::ES + pz * P * P + col) * num_elem + eg] = s;
+        else
+          atomicAdd(diag + off + k * comp_stride, s);
+      }
     }
   }
 }
@@ -85,8 +93,8 @@ template <int P, int Q>
 __global__ void __launch_bounds__(Mass2D<P, Q>::NT) mass2d_diag_kernel(const __grid_constant__ Mat1D<P, Q> m,
                                                                       const int* __restrict__ offs,
                                                                       const double* __restrict__ qd,
-                                                                      double* __restrict__ diag, int num_elem,
-                                                                      int num_comp, int64_t comp_stride) {
+                                                                      double* __restrict__ diag, double* __restrict__ ev,
+                                                                      int num_elem, int num_comp, int64_t comp_stride) {
   using L = Mass2D<P, Q>;
   constexpr int E = L::E;
   __shared__ double s3[Q * P * E];
@@ -117,7 +125,12 @@ __global__ void __launch_bounds__(Mass2D<P, Q>::NT) mass2d_diag_kernel(const __g
 #pragma unroll
       for (int qy = 0; qy < Q; ++qy) s += m.B[qy * P + py] * z[qy];
       const int64_t off = ot[py * (P * E)];
-      for (int k = 0; k < num_comp; ++k) atomicAdd(diag + off + k * comp_stride, s);
+      for (int k = 0; k < num_comp; ++k) {
+        if (ev)
+          ev[(int64_t(k) * L::ES + py * P + col) * num_elem + eg] = s;
+        else
+          atomicAdd(diag + off + k * comp_stride, s);
+      }
     }
   }
 }
@@ -125,8 +138,8 @@ __global__ void __launch_bounds__(Mass2D<P, Q>::NT) mass2d_diag_kernel(const __g
 template <int P, int Q>
 __global__ void __launch_bounds__(128) mass1d_diag_kernel(const __grid_constant__ Mat1D<P, Q> m,
                                                          const int* __restrict__ offs, const double* __restrict__ qd,
-                                                         double* __restrict__ diag, int num_elem, int num_comp,
-                                                         int64_t comp_stride) {
+                                                         double* __restrict__ diag, double* __restrict__ ev,
+                                                         int num_elem, int num_comp, int64_t comp_stride) {
   const int e = threadIdx.x;
   const int64_t tile = blockIdx.x, eg = tile * 128 + e;
   if (eg >= num_elem) return;
@@ -136,92 +149,137 @@ __global__ void __launch_bounds__(128) mass1d_diag_kernel(const __grid_constant_
 #pragma unroll
     for (int qx = 0; qx < Q; ++qx) s += m.B[qx * P + px] * qd[(tile * Q + qx) * 128 + e];
     const int64_t off = offs[(tile * P + px) * 128 + e];
-    for (int k = 0; k < num_comp; ++k) atomicAdd(diag + off + k * comp_stride, s);
-  }
-}
-
-// ---------------------------------------------------------------------------
-// CG vector kernels.  Reductions accumulate in FP64 (warp shuffles, then one
-// atomicAdd per block into a device scalar).
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ double warp_sum(double v) {
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  return v;
-}
-
-template <int N>
-__device__ __forceinline__ void block_sums(double (&v)[N], double* out) {
-  __shared__ double part[N][32];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-#pragma unroll
-  for (int i = 0; i < N; ++i) {
-    v[i] = warp_sum(v[i]);
-    if (lane == 0) part[i][w] = v[i];
-  }
-  __syncthreads();
-  if (w == 0) {
-    const int nw = (blockDim.x + 31) >> 5;
-#pragma unroll
-    for (int i = 0; i < N; ++i) {
-      double s = lane < nw ? part[i][lane] : 0.0;
-      s = warp_sum(s);
-      if (lane == 0) atomicAdd(out + i, s);
+    for (int k = 0; k < num_comp; ++k) {
+      if (ev)
+        ev[(int64_t(k) * P + px) * num_elem + eg] = s;
+      else
+        atomicAdd(diag + off + k * comp_stride, s);
     }
   }
 }
 
-template <class T>
-__global__ void dot_kernel(int64_t n, const T* __restrict__ x, const T* __restrict__ y, double* __restrict__ out) {
-  double v[1] = {0.0};
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
-    v[0] += double(x[i]) * double(y[i]);
-  block_sums<1>(v, out);
-}
 
-// x += a p; r -= a Ap; z = dinv r; out[0] += r.z, out[1] += r.r
+// ---------------------------------------------------------------------------
+// Chronopoulos-Gear PCG vector kernels.  With u = D^-1 r and w = M u:
+//   p = u + beta p;  s = w + beta s;  x += alpha p;  r -= alpha s;
+//   gamma = (r, D^-1 r), rr = (r, r)  -> this kernel's grid reduction;
+//   w = M (D^-1 r), delta = (u, M u)  -> the apply's grid reduction, which
+//   sets beta = gamma / gamma_old and alpha = gamma / (delta - beta gamma / alpha).
+// Every kernel returns at once when the solve has stopped (st->done), so the
+// host can queue several iterations between convergence checks.
+// ---------------------------------------------------------------------------
 template <class T>
-__global__ void cg_update_kernel(int64_t n, double alpha, const T* __restrict__ p, const T* __restrict__ ap,
-                                 const T* __restrict__ dinv, T* __restrict__ x, T* __restrict__ r, T* __restrict__ z,
-                                 double* __restrict__ out) {
-  double v[2] = {0.0, 0.0};
-  const T a = T(alpha);
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
-    x[i] += a * p[i];
-    const T ri = r[i] - a * ap[i];
-    r[i] = ri;
-    const T zi = dinv[i] * ri;
-    z[i] = zi;
-    v[0] += double(ri) * double(zi);
-    v[1] += double(ri) * double(ri);
-  }
-  block_sums<2>(v, out);
-}
-
-// p = z + beta p
-template <class T>
-__global__ void cg_direction_kernel(int64_t n, double beta, const T* __restrict__ z, T* __restrict__ p) {
-  const T b = T(beta);
-  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
-    p[i] = z[i] + b * p[i];
-}
-
-// start: x = 0, r = b * scale (converted), z = dinv r, p = z; out[0] += r.z, out[1] += r.r
-template <class T>
-__global__ void cg_start_kernel(int64_t n, const double* __restrict__ b, double scale, const T* __restrict__ dinv,
-                                T* __restrict__ x, T* __restrict__ r, T* __restrict__ z, T* __restrict__ p,
-                                double* __restrict__ out) {
+__global__ void cg_init_kernel(int64_t n, const double* __restrict__ b, double scale, const T* __restrict__ dinv,
+                               T* __restrict__ x, T* __restrict__ r, T* __restrict__ p, T* __restrict__ sv,
+                               T* __restrict__ w, CgScalars* st, double* part, double rtol, int max_iters) {
   double v[2] = {0.0, 0.0};
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
     const T ri = T(b[i] * scale);
-    const T zi = dinv[i] * ri;
-    x[i] = T(0);
+    x[i] = T(0), p[i] = T(0), sv[i] = T(0), w[i] = T(0);
     r[i] = ri;
-    z[i] = zi;
-    p[i] = zi;
-    v[0] += double(ri) * double(zi);
+    v[0] += double(ri) * double(dinv[i] * ri);
     v[1] += double(ri) * double(ri);
   }
-  block_sums<2>(v, out);
+  grid_sum<2>(v, part, &st->ticket, [&](const double* tot) {
+    st->gamma = tot[0], st->gamma_old = tot[0];
+    st->rr = tot[1], st->rr0 = tot[1];
+    st->tol2 = rtol * rtol * tot[1];
+    st->alpha = 0.0, st->beta = 0.0, st->delta = 0.0;
+    st->iters = 0, st->max_iters = max_iters;
+    st->done = tot[1] > 0.0 ? 0 : 1;
+  });
+}
+
+// 16 bytes of T: the unit of the vectorised update.
+template <class T>
+struct alignas(16) Pack {
+  static constexpr int K = 16 / int(sizeof(T));
+  T a[K];
+};
+
+template <class T, bool VEC>
+__global__ void cg_update_kernel(int64_t n, const T* __restrict__ dinv, T* __restrict__ x, T* __restrict__ r,
+                                 T* __restrict__ p, T* __restrict__ sv, T* __restrict__ w, CgScalars* st,
+                                 double* part) {
+  if (st->done) return;
+  const T a = T(st->alpha), bt = T(st->beta);
+  double v[2] = {0.0, 0.0};
+  auto step = [&](T di, T& ri, T& pi, T& si, T& wi, T& xi) {
+    pi = di * ri + bt * pi;
+    si = wi + bt * si;
+    wi = T(0);
+    xi += a * pi;
+    ri = ri - a * si;
+    v[0] += double(ri) * double(di * ri);
+    v[1] += double(ri) * double(ri);
+  };
+  const int64_t tid = blockIdx.x * int64_t(blockDim.x) + threadIdx.x, stride = int64_t(gridDim.x) * blockDim.x;
+  int64_t head = 0;
+  if constexpr (VEC) {  // every vector 16-byte aligned (checked by the host)
+    using PK = Pack<T>;
+    constexpr int K = PK::K;
+    const int64_t nv = n / K;
+    for (int64_t j = tid; j < nv; j += stride) {
+      const PK D = reinterpret_cast<const PK*>(dinv)[j];
+      PK R = reinterpret_cast<const PK*>(r)[j], Pv = reinterpret_cast<const PK*>(p)[j];
+      PK S = reinterpret_cast<const PK*>(sv)[j], W = reinterpret_cast<const PK*>(w)[j];
+      PK X = reinterpret_cast<const PK*>(x)[j];
+#pragma unroll
+      for (int k = 0; k < K; ++k) step(D.a[k], R.a[k], Pv.a[k], S.a[k], W.a[k], X.a[k]);
+      reinterpret_cast<PK*>(r)[j] = R, reinterpret_cast<PK*>(p)[j] = Pv;
+      reinterpret_cast<PK*>(sv)[j] = S, reinterpret_cast<PK*>(w)[j] = W;
+      reinterpret_cast<PK*>(x)[j] = X;
+    }
+    head = nv * K;
+  }
+  for (int64_t i = head + tid; i < n; i += stride) {
+    T ri = r[i], pi = p[i], si = sv[i], wi = w[i], xi = x[i];
+    step(dinv[i], ri, pi, si, wi, xi);
+    r[i] = ri, p[i] = pi, sv[i] = si, w[i] = wi, x[i] = xi;
+  }
+  grid_sum<2>(v, part, &st->ticket, [&](const double* tot) {
+    st->gamma_old = st->gamma, st->gamma = tot[0];
+    st->rr = tot[1];
+    st->iters += 1;
+    if (tot[1] <= st->tol2)
+      st->done = 1;
+    else if (st->iters >= st->max_iters)
+      st->done = 2;
+  });
+}
+
+// v += the element contributions (deterministic mode) in transpose-map order,
+// the operator's reduction for any T; st == nullptr: outside a solve.
+template <class T>
+__global__ void csr_add_kernel(int num_nodes, int num_elem, int elem_size, int num_comp, int64_t comp_stride,
+                               const int* __restrict__ l_vec_indices, const int* __restrict__ t_offsets,
+                               const int* __restrict__ t_indices, const T* __restrict__ ev, T* __restrict__ v,
+                               const CgScalars* st) {
+  if (st && st->done) return;
+  for (int nd = blockIdx.x * blockDim.x + threadIdx.x; nd < num_nodes; nd += gridDim.x * blockDim.x) {
+    const int64_t l = l_vec_indices[nd];
+    const int t0 = t_offsets[nd], t1 = t_offsets[nd + 1];
+    for (int k = 0; k < num_comp; ++k) {
+      T sum = T(0);
+      for (int t = t0; t < t1; ++t) {
+        const int ti = t_indices[t];
+        const int e = ti / elem_size, i = ti - e * elem_size;
+        sum += ev[(int64_t(k) * elem_size + i) * num_elem + e];
+      }
+      v[l + k * comp_stride] += sum;
+    }
+  }
+}
+
+// diag[off + k*comp_stride] = diag[off] for the components k >= 1 of every
+// element node: the mass diagonal is the same for every component.
+__global__ void broadcast_comp_kernel(int64_t n, const int* __restrict__ offsets, int num_comp, int64_t comp_stride,
+                                      double* __restrict__ diag) {
+  for (int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; t < n; t += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t off = offsets[t];
+    const double d = diag[off];
+    for (int k = 1; k < num_comp; ++k) diag[off + k * comp_stride] = d;
+  }
 }
 
 template <class T>
@@ -236,16 +294,16 @@ __global__ void add_scaled_kernel(int64_t n, double s, const float* __restrict__
     u[i] += s * double(d[i]);
 }
 
-// r = f - Mu; out[0] += r.r
+// r = f - mu (mu == nullptr: r = f); st->res = (r, r)
 __global__ void residual_kernel(int64_t n, const double* __restrict__ f, const double* __restrict__ mu,
-                                double* __restrict__ r, double* __restrict__ out) {
+                                double* __restrict__ r, CgScalars* st, double* part) {
   double v[1] = {0.0};
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
-    const double ri = f[i] - mu[i];
+    const double ri = mu ? f[i] - mu[i] : f[i];
     r[i] = ri;
     v[0] += ri * ri;
   }
-  block_sums<1>(v, out);
+  grid_sum<1>(v, part, &st->ticket, [&](const double* tot) { st->res = tot[0]; });
 }
 
 __global__ void to_float_kernel(int64_t n, const double* __restrict__ in, float* __restrict__ out) {
@@ -254,10 +312,11 @@ __global__ void to_float_kernel(int64_t n, const double* __restrict__ in, float*
 }
 
 // ---------------------------------------------------------------------------
-// dispatch of the diagonal and FP32 apply kernels over the compiled (P, Q) set
+// dispatch of the diagonal and CG apply kernels over the compiled (P, Q) set
 // ---------------------------------------------------------------------------
-using DiagLauncher = void (*)(const MassPlan&, double*, cudaStream_t);
-using Apply32Launcher = void (*)(const MassPlan&, const float*, float*, cudaStream_t);
+using DiagLauncher = void (*)(const MassPlan&, double*, double*, cudaStream_t);
+template <class T>
+using CgApplyLauncher = void (*)(const MassPlan&, const T*, T*, T*, const T*, const ApplyCg<T>&, cudaStream_t);
 
 template <int P, int Q>
 Mat1D<P, Q> squared_mat(const BasisData& b) {
@@ -268,159 +327,265 @@ Mat1D<P, Q> squared_mat(const BasisData& b) {
   return m;
 }
 
-template <int P, int Q>
-Mat1D<P, Q, float> float_mat(const BasisData& b) {
-  Mat1D<P, Q, float> m;
-  for (int i = 0; i < Q * P; ++i) m.B[i] = float(b.interp[i]), m.G[i] = float(b.grad[i]);
-  for (int i = 0; i < Q; ++i) m.W[i] = float(b.q_weight[i]);
+template <int P, int Q, class T>
+Mat1D<P, Q, T> typed_mat(const BasisData& b) {
+  Mat1D<P, Q, T> m;
+  for (int i = 0; i < Q * P; ++i) m.B[i] = T(b.interp[i]), m.G[i] = T(b.grad[i]);
+  for (int i = 0; i < Q; ++i) m.W[i] = T(b.q_weight[i]);
   return m;
 }
 
 template <int P, int Q>
-void launch_diag(const MassPlan& p, double* diag, cudaStream_t s) {
-  const int nc = p.comp_run;
+void launch_diag(const MassPlan& p, double* diag, double* ev, cudaStream_t s) {
+  const int nc = 1;  // component 0; broadcast_comp_kernel copies it to the others
   if (p.dim == 3) {
     using L = Mass3D<P, Q>;
     static std::atomic<uint64_t> smem_set{0};
     set_smem(mass3d_diag_kernel<P, Q>, L::SMEM, smem_set);
     mass3d_diag_kernel<P, Q><<<unsigned(p.n_tiles), L::NT, L::SMEM, s>>>(
-        squared_mat<P, Q>(p.basis), p.offs_t.get(), p.qd_t.get(), diag, p.num_elem, nc, p.comp_stride);
+        squared_mat<P, Q>(p.basis), p.offs_t.get(), p.qd_t.get(), diag, ev, p.num_elem, nc, p.comp_stride);
   } else if (p.dim == 2) {
     mass2d_diag_kernel<P, Q><<<unsigned(p.n_tiles), Mass2D<P, Q>::NT, 0, s>>>(
-        squared_mat<P, Q>(p.basis), p.offs_t.get(), p.qd_t.get(), diag, p.num_elem, nc, p.comp_stride);
+        squared_mat<P, Q>(p.basis), p.offs_t.get(), p.qd_t.get(), diag, ev, p.num_elem, nc, p.comp_stride);
   } else {
-    mass1d_diag_kernel<P, Q><<<unsigned(p.n_tiles), 128, 0, s>>>(squared_mat<P, Q>(p.basis), p.offs_t.get(),
-                                                                  p.qd_t.get(), diag, p.num_elem, nc, p.comp_stride);
+    mass1d_diag_kernel<P, Q><<<unsigned(p.n_tiles), 128, 0, s>>>(
+        squared_mat<P, Q>(p.basis), p.offs_t.get(), p.qd_t.get(), diag, ev, p.num_elem, nc, p.comp_stride);
   }
-  FEM_CUDA_CHECK(cudaGetLastError());
+  FEM_LAUNCH_CHECK();
 }
 
-template <int P, int Q>
-void launch_apply32(const MassPlan& p, const float* u, float* v, cudaStream_t s) {
+// Resident CTAs per SM the persistent CG apply asks for: the most, up to
+// kCgMaxBlocks, that leave a thread kCgMinRegs registers (P <= 5; higher
+// orders need all the registers one CTA per SM leaves).
+constexpr int kCgMaxBlocks = 4, kCgMinRegs = 56;
+constexpr int cg_min_blocks(int threads, int P) {
+  if (P > 5) return 1;
+  for (int b = kCgMaxBlocks; b > 1; --b)
+    if (65536 / (b * threads) >= kCgMinRegs && b * threads <= 2048) return b;
+  return 1;
+}
+
+// CTAs of a persistent launch: SMs x resident CTAs per SM, at most n_tiles.
+template <class K>
+unsigned resident_grid(K kernel, int threads, int smem, int64_t n_tiles) {
+  return unsigned(std::min<int64_t>(resident_ctas(reinterpret_cast<const void*>(kernel), threads, smem), n_tiles));
+}
+
+// w (+)= M (dinv . r) with delta = (dinv . r)^T M (dinv . r) reduced into the
+// solver scalars.  ev != nullptr: element contributions to the E-vector.
+template <int P, int Q, class T, int NCB>
+void launch_cg_apply3(const MassPlan& p, const T* r, T* w, T* ev, const T* qd, const ApplyCg<T>& ext,
+                      cudaStream_t s) {
+  using L = Mass3D<P, Q>;
+  constexpr int smem = NCB * (L::SA + L::SB) * int(sizeof(T));
+  static std::atomic<uint64_t> smem_set{0};
+  const auto kern = mass3d_apply_kernel<P, Q, cg_min_blocks(L::NT, P), T, ApplyCg<T>, NCB>;
+  set_smem(kern, smem, smem_set);
+  kern<<<resident_grid(kern, L::NT, smem, p.n_tiles), L::NT, smem, s>>>(
+      typed_mat<P, Q, T>(p.basis), p.offs_t.get(), qd, r, w, ev, p.num_elem, p.comp_run, p.comp_stride, ext);
+  FEM_LAUNCH_CHECK();
+}
+
+template <int P, int Q, class T>
+void launch_cg_apply(const MassPlan& p, const T* r, T* w, T* ev, const T* qd, const ApplyCg<T>& ext,
+                     cudaStream_t s) {
   if (p.dim == 3) {
-    using L = Mass3D<P, Q>;
-    constexpr int smem = (L::SA + L::SB) * 4;
-    static std::atomic<uint64_t> smem_set{0};
-    set_smem(mass3d_apply_kernel<P, Q, 1, float>, smem, smem_set);
-    mass3d_apply_kernel<P, Q, 1, float><<<unsigned(p.n_tiles), L::NT, smem, s>>>(
-        float_mat<P, Q>(p.basis), p.offs_t.get(), p.qd_t32.get(), u, v, nullptr, p.num_elem, p.comp_run,
-        p.comp_stride);
-  } else if (p.dim == 2) {
-    using L = Mass2D<P, Q>;
-    constexpr int smem = (L::S1 + L::S3) * 4;
-    mass2d_apply_kernel<P, Q, float><<<unsigned(p.n_tiles), L::NT, smem, s>>>(
-        float_mat<P, Q>(p.basis), p.offs_t.get(), p.qd_t32.get(), u, v, nullptr, p.num_elem, p.comp_run,
-        p.comp_stride);
-  } else {
-    mass1d_apply_kernel<P, Q, float><<<unsigned(p.n_tiles), 128, 0, s>>>(
-        float_mat<P, Q>(p.basis), p.offs_t.get(), p.qd_t32.get(), u, v, nullptr, p.num_elem, p.comp_run,
-        p.comp_stride);
+    // components batched through the phases (measured faster for 2 and 3
+    // components in both precisions) where shared memory allows
+    constexpr int smem1 = (Mass3D<P, Q>::SA + Mass3D<P, Q>::SB) * int(sizeof(T));
+    if constexpr (3 * smem1 <= kMaxSmemPerCta) {
+      if (p.comp_run == 3) return launch_cg_apply3<P, Q, T, 3>(p, r, w, ev, qd, ext, s);
+    }
+    if constexpr (2 * smem1 <= kMaxSmemPerCta) {
+      if (p.comp_run == 2) return launch_cg_apply3<P, Q, T, 2>(p, r, w, ev, qd, ext, s);
+    }
+    return launch_cg_apply3<P, Q, T, 1>(p, r, w, ev, qd, ext, s);
   }
-  FEM_CUDA_CHECK(cudaGetLastError());
+  if (p.dim == 2) {
+    using L = Mass2D<P, Q>;
+    constexpr int smem = (L::S1 + L::S3) * int(sizeof(T));
+    static std::atomic<uint64_t> smem_set{0};
+    const auto kern = mass2d_apply_kernel<P, Q, T, ApplyCg<T>>;
+    set_smem(kern, smem, smem_set);
+    kern<<<resident_grid(kern, L::NT, smem, p.n_tiles), L::NT, smem, s>>>(
+        typed_mat<P, Q, T>(p.basis), p.offs_t.get(), qd, r, w, ev, p.num_elem, p.comp_run, p.comp_stride, ext);
+  } else {
+    const auto kern = mass1d_apply_kernel<P, Q, T, ApplyCg<T>>;
+    kern<<<resident_grid(kern, 128, 0, p.n_tiles), 128, 0, s>>>(
+        typed_mat<P, Q, T>(p.basis), p.offs_t.get(), qd, r, w, ev, p.num_elem, p.comp_run, p.comp_stride, ext);
+  }
+  FEM_LAUNCH_CHECK();
 }
 
 constexpr int kSolveMinP = 2, kSolveMaxP = 8, kSolveQSpan = 3;
 
+struct SolveDispatch {
+  DiagLauncher diag[kSolveMaxP + 1][kSolveQSpan] = {};
+  CgApplyLauncher<double> cg64[kSolveMaxP + 1][kSolveQSpan] = {};
+  CgApplyLauncher<float> cg32[kSolveMaxP + 1][kSolveQSpan] = {};
+};
+
 template <int P, int DQ>
 struct SolveTable {
-  static void fill(DiagLauncher (*dg)[kSolveQSpan], Apply32Launcher (*ap)[kSolveQSpan]) {
-    dg[P][DQ] = launch_diag<P, P + DQ>;
-    ap[P][DQ] = launch_apply32<P, P + DQ>;
+  static void fill(SolveDispatch& d) {
+    d.diag[P][DQ] = launch_diag<P, P + DQ>;
+    d.cg64[P][DQ] = launch_cg_apply<P, P + DQ, double>;
+    d.cg32[P][DQ] = launch_cg_apply<P, P + DQ, float>;
     if constexpr (DQ + 1 < kSolveQSpan)
-      SolveTable<P, DQ + 1>::fill(dg, ap);
+      SolveTable<P, DQ + 1>::fill(d);
     else if constexpr (P + 1 <= kSolveMaxP)
-      SolveTable<P + 1, 0>::fill(dg, ap);
+      SolveTable<P + 1, 0>::fill(d);
   }
 };
 
-struct SolveDispatch {
-  DiagLauncher diag[kSolveMaxP + 1][kSolveQSpan] = {};
-  Apply32Launcher apply32[kSolveMaxP + 1][kSolveQSpan] = {};
-  SolveDispatch() { SolveTable<kSolveMinP, 0>::fill(diag, apply32); }
-};
-
 const SolveDispatch& solve_dispatch() {
-  static SolveDispatch d;
+  static const SolveDispatch d = [] {
+    SolveDispatch t;
+    SolveTable<kSolveMinP, 0>::fill(t);
+    return t;
+  }();
   return d;
 }
 
 inline int red_grid(int64_t n) { return int(std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 8))); }
 
-// The plan's solver state: diagonal, its inverse in both precisions, the FP32
-// copy of qdata, CG vectors, and the device scalars of the reductions.
+bool deterministic(const MassPlan& p) { return p.scatter_mode != FEM_B200_SCATTER_ATOMIC; }
+
+// diag = the assembled diagonal (zeroed first); transpose-map order in
+// deterministic plans, atomics otherwise.  Component 0 is assembled and
+// copied to the others, so every component of a node holds the same bits
+// (the CG apply reads one scale per node).
+void assemble_diagonal(MassPlan& p, double* diag, cudaStream_t s) {
+  FEM_CUDA_CHECK(cudaMemsetAsync(diag, 0, size_t(p.l_size) * sizeof(double), s));
+  const DiagLauncher launch = solve_dispatch().diag[p.P][p.Q - p.P];
+  const RestrictionData& r = *p.r;
+  if (!deterministic(p)) {
+    launch(p, diag, nullptr, s);
+  } else {
+    launch(p, diag, p.evec.get(), s);
+    csr_add_kernel<double><<<grid_for(r.num_nodes, 256), 256, 0, s>>>(
+        r.num_nodes, p.num_elem, p.es, 1, p.comp_stride, r.l_vec_indices.get(), r.t_offsets.get(),
+        r.t_indices.get(), p.evec.get(), diag, nullptr);
+    FEM_LAUNCH_CHECK();
+  }
+  if (p.comp_run > 1) {
+    const int64_t n = int64_t(p.num_elem) * p.es;
+    broadcast_comp_kernel<<<grid_for(n, 256), 256, 0, s>>>(n, r.offsets.get(), p.comp_run, p.comp_stride, diag);
+    FEM_LAUNCH_CHECK();
+  }
+}
+
+// The plan's solver state: diagonal and its inverse, FP32 copies of qdata
+// and dinv, Krylov vectors, reduction partials and the device scalars.
 void ensure_solver_state(MassPlan& p, bool fp32, cudaStream_t s) {
   const size_t n = size_t(p.l_size);
   if (p.diag.size() != n) {
     p.diag.alloc(n);
-    FEM_CUDA_CHECK(cudaMemsetAsync(p.diag.get(), 0, n * sizeof(double), s));
-    solve_dispatch().diag[p.P][p.Q - p.P](p, p.diag.get(), s);
+    assemble_diagonal(p, p.diag.get(), s);
     p.dinv.alloc(n);
     invert_kernel<double><<<red_grid(int64_t(n)), 256, 0, s>>>(int64_t(n), p.diag.get(), p.dinv.get());
-    FEM_CUDA_CHECK(cudaGetLastError());
-    p.cg_r.alloc(n), p.cg_z.alloc(n), p.cg_p.alloc(n), p.cg_ap.alloc(n);
-    p.red.alloc(4);
+    FEM_LAUNCH_CHECK();
+    p.cg_r.alloc(n), p.cg_p.alloc(n), p.cg_s.alloc(n), p.cg_w.alloc(n);
+    p.part.alloc(2 * size_t(std::max<int64_t>(p.n_tiles, 148 * 8)));
+    p.cg_st.alloc(1);
+    FEM_CUDA_CHECK(cudaMemsetAsync(p.cg_st.get(), 0, sizeof(CgScalars), s));
+    p.cg_host.alloc(1);
   }
   if (fp32 && p.qd_t32.size() != p.qd_t.size()) {
     p.qd_t32.alloc(p.qd_t.size());
     to_float_kernel<<<red_grid(int64_t(p.qd_t.size())), 256, 0, s>>>(int64_t(p.qd_t.size()), p.qd_t.get(),
                                                                     p.qd_t32.get());
-    FEM_CUDA_CHECK(cudaGetLastError());
+    FEM_LAUNCH_CHECK();
     p.dinv32.alloc(n);
     invert_kernel<float><<<red_grid(int64_t(n)), 256, 0, s>>>(int64_t(n), p.diag.get(), p.dinv32.get());
-    FEM_CUDA_CHECK(cudaGetLastError());
-    p.f_r.alloc(n), p.f_z.alloc(n), p.f_p.alloc(n), p.f_ap.alloc(n), p.f_x.alloc(n);
+    FEM_LAUNCH_CHECK();
+    p.f_r.alloc(n), p.f_p.alloc(n), p.f_s.alloc(n), p.f_w.alloc(n), p.f_x.alloc(n);
+    if (deterministic(p)) p.evec32.alloc(p.evec.size());
   }
 }
 
-// Reads the first k reduction scalars (synchronises the stream) and clears them.
-void read_reductions(MassPlan& p, double* out, int k, cudaStream_t s) {
-  FEM_CUDA_CHECK(cudaMemcpyAsync(out, p.red.get(), k * sizeof(double), cudaMemcpyDeviceToHost, s));
-  FEM_CUDA_CHECK(cudaMemsetAsync(p.red.get(), 0, 4 * sizeof(double), s));
+// The host's copy of the device scalars (synchronises the stream).
+const CgScalars& read_scalars(MassPlan& p, cudaStream_t s) {
+  FEM_CUDA_CHECK(cudaMemcpyAsync(p.cg_host.get(), p.cg_st.get(), sizeof(CgScalars), cudaMemcpyDeviceToHost, s));
   FEM_CUDA_CHECK(cudaStreamSynchronize(s));
+  return *p.cg_host.get();
 }
 
-struct CgResult {
-  int iterations = 0;
-  double rel = 0.0;  // final recursive residual / initial
+inline bool aligned16(const void* ptr) { return (reinterpret_cast<uintptr_t>(ptr) & 15) == 0; }
+
+template <class T>
+struct Krylov {
+  T *x, *r, *p, *s, *w, *ev;
+  const T *dinv, *qd;
+  CgApplyLauncher<T> apply;
 };
 
-// Jacobi PCG on `apply` for A x = b*scale, x starting at 0, until
-// ||r|| <= rtol ||r0|| or max_it.  T = double (FP64) or float (FP32 vectors).
-template <class T, class ApplyFn>
-CgResult pcg(MassPlan& p, ApplyFn apply, const double* b, double scale, const T* dinv, T* x, T* r, T* z, T* pv, T* ap,
-             double rtol, int max_it, cudaStream_t s) {
+template <class T>
+void cg_apply(MassPlan& p, const Krylov<T>& k, cudaStream_t s) {
+  const ApplyCg<T> ext{k.dinv, p.part.get(), p.cg_st.get()};
+  if (!deterministic(p)) {
+    k.apply(p, k.r, k.w, nullptr, k.qd, ext, s);
+    return;
+  }
+  const RestrictionData& r = *p.r;
+  k.apply(p, k.r, nullptr, k.ev, k.qd, ext, s);
+  csr_add_kernel<T><<<grid_for(r.num_nodes, 256), 256, 0, s>>>(r.num_nodes, p.num_elem, p.es, p.comp_run,
+                                                               p.comp_stride, r.l_vec_indices.get(),
+                                                               r.t_offsets.get(), r.t_indices.get(), k.ev, k.w,
+                                                               p.cg_st.get());
+  FEM_LAUNCH_CHECK();
+}
+
+// Jacobi PCG on M x = b * scale from x = 0 until ||r|| <= rtol ||r0|| or
+// max_it residual updates.  The host queues iterations in growing batches and
+// reads the scalars between batches; kernels queued after the stop return at
+// once.  Returns the final scalars.
+template <class T>
+CgScalars krylov_solve(MassPlan& p, const Krylov<T>& k, const double* b, double scale, double rtol, int max_it,
+                       cudaStream_t s) {
   const int64_t n = p.l_size;
   const int g = red_grid(n);
-  double red[2];
-  FEM_CUDA_CHECK(cudaMemsetAsync(p.red.get(), 0, 4 * sizeof(double), s));
-  cg_start_kernel<T><<<g, 256, 0, s>>>(n, b, scale, dinv, x, r, z, pv, p.red.get());
-  FEM_CUDA_CHECK(cudaGetLastError());
-  read_reductions(p, red, 2, s);
-  double rz = red[0];
-  const double r0 = std::sqrt(red[1]);
-  CgResult res;
-  if (r0 == 0.0) return res;
-  double rnorm = r0;
-  for (int it = 0; it < max_it && rnorm > rtol * r0; ++it) {
-    apply(pv, ap);
-    dot_kernel<T><<<g, 256, 0, s>>>(n, pv, ap, p.red.get());
-    FEM_CUDA_CHECK(cudaGetLastError());
-    read_reductions(p, red, 1, s);
-    if (!(red[0] > 0.0)) throw cuda_error("mass solve: the operator is not positive definite on this vector");
-    const double alpha = rz / red[0];
-    cg_update_kernel<T><<<g, 256, 0, s>>>(n, alpha, pv, ap, dinv, x, r, z, p.red.get());
-    FEM_CUDA_CHECK(cudaGetLastError());
-    read_reductions(p, red, 2, s);
-    const double beta = red[0] / rz;
-    rz = red[0];
-    rnorm = std::sqrt(red[1]);
-    cg_direction_kernel<T><<<g, 256, 0, s>>>(n, beta, z, pv);
-    FEM_CUDA_CHECK(cudaGetLastError());
-    res.iterations = it + 1;
+  cg_init_kernel<T><<<g, 256, 0, s>>>(n, b, scale, k.dinv, k.x, k.r, k.p, k.s, k.w, p.cg_st.get(), p.part.get(),
+                                      rtol, max_it);
+  FEM_LAUNCH_CHECK();
+  cg_apply<T>(p, k, s);
+  const bool vec = aligned16(k.dinv) && aligned16(k.x) && aligned16(k.r) && aligned16(k.p) && aligned16(k.s) &&
+                   aligned16(k.w);
+  int batch = 4;
+  for (int queued = 0;; queued += batch, batch = std::min(batch * 2, 32)) {
+    for (int j = 0; j < batch; ++j) {
+      if (vec)
+        cg_update_kernel<T, true><<<g, 256, 0, s>>>(n, k.dinv, k.x, k.r, k.p, k.s, k.w, p.cg_st.get(), p.part.get());
+      else
+        cg_update_kernel<T, false><<<g, 256, 0, s>>>(n, k.dinv, k.x, k.r, k.p, k.s, k.w, p.cg_st.get(),
+                                                     p.part.get());
+      FEM_LAUNCH_CHECK();
+      cg_apply<T>(p, k, s);
+    }
+    const CgScalars& st = read_scalars(p, s);
+    if (st.done) break;
+    if (queued > max_it + 64) throw cuda_error("mass solve: the device iteration count did not advance");
   }
-  res.rel = rnorm / r0;
-  return res;
+  const CgScalars st = *p.cg_host.get();
+  if (st.done == 3 && st.iters == 0)
+    throw cuda_error("mass solve: breakdown, (u, M u) <= 0: the operator is not positive definite on this "
+                     "right-hand side");
+  return st;
 }
+
+// r = f - M u (cg_w: scratch for M u; u == nullptr: r = f); returns ||r||.
+double outer_residual(MassPlan& p, const double* f, const double* u, cudaStream_t s) {
+  const int64_t n = p.l_size;
+  if (u) mass_apply_impl(p, u, p.cg_w.get(), true, s);
+  residual_kernel<<<red_grid(n), 256, 0, s>>>(n, f, u ? p.cg_w.get() : nullptr, p.cg_r.get(), p.cg_st.get(),
+                                               p.part.get());
+  FEM_LAUNCH_CHECK();
+  return std::sqrt(read_scalars(p, s).res);
+}
+
+// The FP32 inner solve's relative tolerance: what the last cycle still needs
+// (with a factor 2 margin), but not below what FP32 Krylov vectors attain.
+constexpr double kInnerFloor = 5e-6;
 
 }  // namespace fem_b200
 
@@ -434,9 +599,7 @@ int fem_b200_mass_diagonal(fem_b200_mass op, double* diag, int64_t n, void* stre
     MassPlan& p = *op->d;
     require(n == p.l_size && diag, "mass diagonal: diag must have l_size entries");
     DeviceGuard g(p.device);
-    cudaStream_t s = as_stream(stream);
-    FEM_CUDA_CHECK(cudaMemsetAsync(diag, 0, size_t(n) * sizeof(double), s));
-    solve_dispatch().diag[p.P][p.Q - p.P](p, diag, s);
+    assemble_diagonal(p, diag, as_stream(stream));
   });
 }
 
@@ -457,62 +620,42 @@ int fem_b200_mass_solve(fem_b200_mass op, const double* f, int64_t n_f, double* 
           "FEM_B200_QF_APPLY_MASS_VECTOR for a multi-component solve");
     DeviceGuard g(p.device);
     cudaStream_t s = as_stream(stream);
-    const int64_t n = p.l_size;
-    const int grid = red_grid(n);
-    ensure_solver_state(p, precision == FEM_B200_SOLVE_FP32_IR, s);
+    const bool fp32 = precision == FEM_B200_SOLVE_FP32_IR;
+    ensure_solver_state(p, fp32, s);
+    const SolveDispatch& d = solve_dispatch();
+    const int di = p.Q - p.P;
     int total_it = 0, outer = 0;
-    double red[2];
-    // ||f||
-    FEM_CUDA_CHECK(cudaMemsetAsync(p.red.get(), 0, 4 * sizeof(double), s));
-    dot_kernel<double><<<grid, 256, 0, s>>>(n, f, f, p.red.get());
-    FEM_CUDA_CHECK(cudaGetLastError());
-    read_reductions(p, red, 1, s);
-    const double nf = std::sqrt(red[0]);
-    if (nf == 0.0) {
-      FEM_CUDA_CHECK(cudaMemsetAsync(u, 0, size_t(n) * sizeof(double), s));
-      if (iterations) *iterations = 0;
-      if (refinements) *refinements = 0;
-      if (rel_residual) *rel_residual = 0.0;
-      FEM_CUDA_CHECK(cudaStreamSynchronize(s));
-      return;
-    }
-    auto apply64 = [&](const double* x, double* y) { mass_apply_impl(p, x, y, true, s); };
-    if (precision == FEM_B200_SOLVE_FP64) {
-      CgResult r = pcg<double>(p, apply64, f, 1.0, p.dinv.get(), u, p.cg_r.get(), p.cg_z.get(), p.cg_p.get(),
-                               p.cg_ap.get(), rtol, max_iter, s);
-      total_it = r.iterations;
+    double nf = 0.0, nr = 0.0;
+    if (!fp32) {
+      const Krylov<double> k{u, p.cg_r.get(), p.cg_p.get(), p.cg_s.get(), p.cg_w.get(), p.evec.get(),
+                             p.dinv.get(), p.qd_t.get(), d.cg64[p.P][di]};
+      const CgScalars st = krylov_solve<double>(p, k, f, 1.0, rtol, max_iter, s);
+      total_it = st.iters;
+      nf = std::sqrt(st.rr0);
+      nr = outer_residual(p, f, u, s);  // the true FP64 residual
     } else {
-      // FP64 outer loop: r = f - M u (FP64), correction from FP32 PCG on r/||r||
-      auto apply32 = [&](const float* x, float* y) {
-        FEM_CUDA_CHECK(cudaMemsetAsync(y, 0, size_t(n) * sizeof(float), s));
-        solve_dispatch().apply32[p.P][p.Q - p.P](p, x, y, s);
-      };
-      FEM_CUDA_CHECK(cudaMemsetAsync(u, 0, size_t(n) * sizeof(double), s));
-      FEM_CUDA_CHECK(cudaMemcpyAsync(p.cg_r.get(), f, size_t(n) * sizeof(double), cudaMemcpyDeviceToDevice, s));
-      double nr = nf;
-      const double inner_rtol = 1e-5;
-      for (outer = 0; outer < 50 && nr > rtol * nf && total_it < max_iter; ++outer) {
-        CgResult r = pcg<float>(p, apply32, p.cg_r.get(), 1.0 / nr, p.dinv32.get(), p.f_x.get(), p.f_r.get(),
-                                p.f_z.get(), p.f_p.get(), p.f_ap.get(), inner_rtol, max_iter - total_it, s);
-        total_it += r.iterations;
-        add_scaled_kernel<<<grid, 256, 0, s>>>(n, nr, p.f_x.get(), u);
-        FEM_CUDA_CHECK(cudaGetLastError());
-        apply64(u, p.cg_ap.get());
-        residual_kernel<<<grid, 256, 0, s>>>(n, f, p.cg_ap.get(), p.cg_r.get(), p.red.get());
-        FEM_CUDA_CHECK(cudaGetLastError());
-        read_reductions(p, red, 1, s);
-        nr = std::sqrt(red[0]);
+      // FP64 outer loop: r = f - M u in FP64, correction from FP32 PCG on r / ||r||.
+      nf = outer_residual(p, f, nullptr, s);
+      FEM_CUDA_CHECK(cudaMemsetAsync(u, 0, size_t(p.l_size) * sizeof(double), s));
+      nr = nf;
+      const Krylov<float> k{p.f_x.get(), p.f_r.get(), p.f_p.get(), p.f_s.get(), p.f_w.get(), p.evec32.get(),
+                            p.dinv32.get(), p.qd_t32.get(), d.cg32[p.P][di]};
+      while (nr > rtol * nf && total_it < max_iter && outer < 50) {
+        const double inner = std::min(0.5, std::max(kInnerFloor, 0.5 * rtol * nf / nr));
+        const CgScalars st = krylov_solve<float>(p, k, p.cg_r.get(), 1.0 / nr, inner, max_iter - total_it, s);
+        total_it += st.iters;
+        ++outer;
+        add_scaled_kernel<<<red_grid(p.l_size), 256, 0, s>>>(p.l_size, nr, p.f_x.get(), u);
+        FEM_LAUNCH_CHECK();
+        const double prev = nr;
+        nr = outer_residual(p, f, u, s);
+        if (!(nr < prev)) break;  // no progress: the FP32 solve has stalled
       }
     }
-    // the true FP64 residual ||f - M u|| / ||f||
-    apply64(u, p.cg_ap.get());
-    residual_kernel<<<grid, 256, 0, s>>>(n, f, p.cg_ap.get(), p.cg_r.get(), p.red.get());
-    FEM_CUDA_CHECK(cudaGetLastError());
-    read_reductions(p, red, 1, s);
     check_status(p);
     if (iterations) *iterations = total_it;
     if (refinements) *refinements = outer;
-    if (rel_residual) *rel_residual = std::sqrt(red[0]) / nf;
+    if (rel_residual) *rel_residual = nf > 0.0 ? nr / nf : 0.0;
   });
 }
 

@@ -188,3 +188,21 @@ def test_component0_apply_mass_is_not_solvable(fem, cuda):
     f = torch.ones(l_size, dtype=torch.float64, device=cuda)
     with pytest.raises(fem.FemUnsupported):
         op.solve(f, torch.empty_like(f))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32_ir"])
+def test_deterministic_solve_is_bitwise_reproducible(fem, cuda, precision):
+    """Deterministic plans: transpose-map scatter and fixed-order grid
+    reductions, so a repeated solve reproduces every bit."""
+    import torch
+    m = box_mesh((7, 6, 5), 4, seed=2)
+    op, _, _, _, l_size = operator(fem, cuda, m, 5, nc=2, scatter=1)
+    f = dev(random_vector(l_size, 31), cuda)
+    out = []
+    for _ in range(3):
+        u = torch.empty_like(f)
+        info = op.solve(f, u, rtol=1e-11, precision=precision)
+        out.append((host(u), info))
+    for u_h, info in out[1:]:
+        assert np.array_equal(u_h, out[0][0])
+        assert info == out[0][1]
