@@ -484,6 +484,128 @@ def run_solve(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# batched uneven meshes: 512 independent 2D/3D boxes (d = 2 or 3 at 50/50,
+# elements log-uniform in [4^d, 48^d], P uniform in 2..6, Q = P+1, num_comp
+# uniform in 1..3), one graph launch per step, FP64 and FP32 (extra lines)
+# ---------------------------------------------------------------------------
+def batch_specs(n, seed):
+    rng = np.random.default_rng([seed, 4])
+    specs = []
+    for _ in range(n):
+        d = 2 if rng.random() < 0.5 else 3
+        side = int(round(float(np.exp(rng.uniform(np.log(4), np.log(48))))))
+        P = int(rng.integers(2, 7))
+        nc = int(rng.integers(1, 4))
+        specs.append((d, (side,) * d, P, nc))
+    return specs
+
+
+def make_batch_ops(n_meshes, dev):
+    """The batch workload's operators and inputs: (specs, ops, us, dofs,
+    algorithmic bytes in FP64, in FP32)."""
+    import torch
+    import fe_demo_cpp_b200 as fem
+    from fe_demo_cpp_b200.mesh import box_mesh
+    from fe_demo_cpp_b200.mesh_gpu import box_mesh_device
+    specs = batch_specs(n_meshes, SEED)
+    ops, us, abytes64, abytes32, dofs = [], [], 0, 0, 0
+    for i, (d, shape, Pp, nc) in enumerate(specs):
+        Qq = Pp + 1
+        if d == 3:
+            m = box_mesh_device(shape, Pp, seed=SEED + i, device=dev)
+            offs, coords = m.offsets.cpu().numpy(), m.coords
+        else:
+            m = box_mesh(shape, Pp, seed=SEED + i)
+            offs, coords = m.offsets, torch.from_numpy(m.coords).to(dev)
+        N, ne = m.num_nodes, m.num_elem
+        rx = fem.Restriction(ne, Pp**d, d, N, d * N, offs)
+        qd = torch.empty(Qq**d * ne, dtype=torch.float64, device=dev)
+        fem.mass_build(rx, fem.Basis(d, d, Pp, Qq), coords, qd)
+        del rx, coords
+        op = fem.MassOperator(fem.Restriction(ne, Pp**d, nc, N, nc * N, offs), fem.Basis(d, nc, Pp, Qq), qd,
+                              fem.QF.apply_mass_vector)
+        del qd
+        ops.append(op)
+        g = torch.Generator(device=dev).manual_seed(SEED * 1000 + i)
+        us.append(torch.rand(nc * N, dtype=torch.float64, device=dev, generator=g) * 2 - 1)
+        dofs += nc * N
+        abytes64 += ne * (4 * Pp**d + 8 * Qq**d) + 16 * nc * N
+        abytes32 += ne * (4 * Pp**d + 4 * Qq**d) + 8 * nc * N
+    return specs, ops, us, dofs, abytes64, abytes32
+
+
+def run_batch(args):
+    import torch
+    import fe_demo_cpp_b200 as fem
+    from fe_demo_cpp_b200.build import build
+    from fe_demo_cpp_b200.telemetry import ClockSampler
+
+    build()
+    dev = torch.device("cuda", 0)
+    specs, ops, us, dofs, abytes64, abytes32 = make_batch_ops(args.batch_meshes, dev)
+    torch.cuda.synchronize()
+    peak, _ = measured_peaks()
+    n3 = sum(1 for sp in specs if sp[0] == 3)
+    cfg = {"meshes": len(specs), "meshes_3d": n3, "meshes_2d": len(specs) - n3, "dofs": dofs,
+           "elements": int(sum(int(np.prod(sp[1])) for sp in specs)),
+           "spec": "d in {2,3} 50/50, elements log-uniform in [4^d, 48^d] (cubic/square boxes), P uniform 2..6, "
+                   "Q=P+1, num_comp uniform 1..3 (vector mass), seeded perturbation, u ~ U[-1,1]",
+           "l2": "inputs larger than L2; no flush"}
+    K = args.batch_steps
+    sampler = ClockSampler(0).start()
+
+    def timed(fn, steps):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    results = []
+    # per-operator loop (the unbatched path: one public apply per mesh)
+    vs = [torch.empty_like(u) for u in us]
+
+    def loop():
+        for op, u, v in zip(ops, us, vs):
+            op.apply(u, v)
+    results.append(("fp64", "per-operator loop", timed(loop, max(2, K // 4)), None))
+    for prec in ("fp64", "fp32"):
+        uu = us if prec == "fp64" else [u.float() for u in us]
+        vv = [torch.empty_like(u) for u in uu]
+        b = fem.Batch(ops, prec)
+        b.bind(uu, vv)
+        results.append((prec, "batch, kernels launched directly", timed(lambda: b.apply(graph=False), K), b.info()))
+        results.append((prec, "batch, one graph launch", timed(lambda: b.apply(graph=True), K), b.info()))
+        b.autotune(reps=3)
+        results.append((prec, "batch, kernels launched directly, autotuned", timed(lambda: b.apply(graph=False), K),
+                        b.info()))
+        results.append((prec, "batch, one graph launch, autotuned", timed(lambda: b.apply(graph=True), K), b.info()))
+        if prec == "fp64":
+            # parity guard: the batch result against each operator's own apply
+            worst = 0.0
+            for op, u, v in list(zip(ops, uu, vv))[:: max(1, len(ops) // 32)]:
+                w = torch.empty_like(u)
+                op.apply(u, w)
+                worst = max(worst, float((v - w).abs().max() / w.abs().max()))
+            assert worst <= 1e-13, worst
+        del b, uu, vv
+    clocks = sampler.stop()
+    for prec, mode, ms, info in results:
+        ab = abytes64 if prec == "fp64" else abytes32
+        print(json.dumps({"batch": "mass_apply", "precision": prec, "mode": mode, "metric": "GDoF/s batched apply",
+                          "value": dofs / (ms * 1e-3) / 1e9, "unit": "GDoF/s", "ms_per_step": ms, "steps": K,
+                          "roofline": {"bound": "hbm", "achieved_gbs": ab / (ms * 1e-3) / 1e9, "peak_gbs": peak,
+                                       "frac": ab / (ms * 1e-3) / 1e9 / peak, "algorithmic_bytes": ab},
+                          "batch_info": info, "config": cfg, "clocks": clocks}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -504,7 +626,12 @@ def main():
     ap.add_argument("--solve-rtol", type=float, default=1e-10)
     ap.add_argument("--solve-steps", type=int, default=20)
     ap.add_argument("--solve-scatter", type=int, default=0, help="0 atomic, 1 deterministic")
+    ap.add_argument("--batch", action="store_true", help="512 uneven meshes in one graph, FP64 and FP32 (extra lines)")
+    ap.add_argument("--batch-meshes", type=int, default=512)
+    ap.add_argument("--batch-steps", type=int, default=20)
     args = ap.parse_args()
+    if args.batch:
+        return run_batch(args)
     if args.sweep:
         return run_sweep(args)
     if args.solve:

@@ -10,6 +10,7 @@ from ._lib import FemError, FemUnsupported, LIB_PATH, load  # noqa: F401
 from .api import (  # noqa: F401
     QF,
     Basis,
+    Batch,
     ContractMode,
     EvalMode,
     KernelVariant,

@@ -315,3 +315,48 @@ class MassOperator(_Handle):
     def check(self, stream=None) -> None:
         """Synchronise and raise if a device-side wait of the plan's kernels ran out."""
         call("fem_b200_mass_check", self.h, _stream(stream))
+
+
+class Batch(_Handle):
+    """Many mass operators applied together, v_i = M_i u_i, as one captured
+    CUDA graph (fem_b200_batch_*).  precision 'fp64' or 'fp32' (FP32 vectors
+    and qdata).  The operators must outlive the batch."""
+    _destroy = "fem_b200_batch_destroy"
+
+    def __init__(self, ops, precision="fp64"):
+        super().__init__()
+        if precision not in ("fp64", "fp32"):
+            raise ValueError("batch precision must be 'fp64' or 'fp32'")
+        self.ops = list(ops)  # keeps the operators alive
+        self.precision = precision
+        arr = (C.c_void_p * len(self.ops))(*[op.h.value for op in self.ops])
+        call("fem_b200_batch_create", C.addressof(arr), len(self.ops), {"fp64": 0, "fp32": 1}[precision],
+             C.addressof(self.h))
+        self._bound = None
+
+    def bind(self, us, vs, stream=None) -> None:
+        dt = "float64" if self.precision == "fp64" else "float32"
+        assert len(us) == len(self.ops) and len(vs) == len(self.ops)
+        for op, u, v in zip(self.ops, us, vs):
+            _check_dev(u, dt)
+            _check_dev(v, dt)
+            if _n(u) != op.l_size or _n(v) != op.l_size:
+                raise ValueError("batch bind: vector sizes must equal each operator's l_size")
+        ua = (C.c_void_p * len(us))(*[_ptr(u) for u in us])
+        va = (C.c_void_p * len(vs))(*[_ptr(v) for v in vs])
+        call("fem_b200_batch_bind", self.h, C.addressof(ua), C.addressof(va), _stream(stream))
+        self._bound = (list(us), list(vs))  # keeps the bound tensors alive
+
+    def apply(self, graph=True, stream=None) -> None:
+        call("fem_b200_batch_apply", self.h, int(bool(graph)), _stream(stream))
+
+    def autotune(self, reps=5, stream=None) -> None:
+        call("fem_b200_batch_autotune", self.h, int(reps), _stream(stream))
+
+    def info(self) -> dict:
+        nc, gk, pc = C.c_int(0), C.c_int(0), C.c_int(0)
+        tiles, dofs = C.c_int64(0), C.c_int64(0)
+        call("fem_b200_batch_info", self.h, C.addressof(nc), C.addressof(tiles), C.addressof(dofs),
+             C.addressof(gk), C.addressof(pc))
+        return {"classes": nc.value, "tiles": tiles.value, "dofs": dofs.value, "graph_kernels": gk.value,
+                "persistent_classes": pc.value}

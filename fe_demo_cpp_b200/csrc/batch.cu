@@ -1,0 +1,500 @@
+// Batched mass apply over many independent meshes of uneven size and order
+// (sm_100a): v_i = M_i u_i for every operator of the batch, replayed as ONE
+// captured CUDA graph.
+//
+// The meshes are grouped into classes of equal (dim, P, Q, components, basis);
+// each class is one kernel over a device table of (mesh, tile) pairs, with
+// the per-mesh pointers and sizes in a device descriptor table, so the
+// per-tile work is the single-mesh kernels' tile functions (mass3d_tile,
+// mass2d_tile, mass1d_element) unchanged.  The graph holds one kernel that
+// zeroes every v_i, then the class kernels on parallel branches (classes
+// write disjoint outputs).  Rebinding the u_i / v_i pointers rewrites the
+// descriptor table and keeps the graph.  Each class's schedule -- one CTA
+// per tile, or a persistent grid of resident CTAs -- is chosen by timing
+// both (fem_b200_batch_autotune).
+//
+// The reference applies one operator at a time (src/operator.cpp:148-182);
+// the batch is the same operator over many meshes with no counterpart there.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <tuple>
+#include <type_traits>
+
+#include "plan.hpp"
+
+namespace fem_b200 {
+
+// One mesh of a batch, read by the device.
+template <class T>
+struct BatchMesh {
+  const int* offs;  // the plan's tiled offsets
+  const T* qd;      // its tiled qdata in T
+  const T* u;
+  T* v;
+  int64_t l_size;
+  int64_t comp_stride;
+  int num_elem, comp_run;
+};
+
+template <class T>
+__global__ void batch_zero_kernel(const BatchMesh<T>* __restrict__ meshes) {
+  const BatchMesh<T> mm = meshes[blockIdx.y];
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < mm.l_size; i += int64_t(gridDim.x) * blockDim.x)
+    mm.v[i] = T(0);
+}
+
+__global__ void batch_to_float_kernel(int64_t n, const double* __restrict__ in, float* __restrict__ out) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    out[i] = float(in[i]);
+}
+
+// Tiles g = blockIdx.x, +gridDim.x, ... of a class; tiles[g] = (mesh, tile).
+template <int P, int Q, int MINB, class T, int NCB>
+__global__ void __launch_bounds__(Mass3D<P, Q>::NT, MINB)
+    mass3d_batch_kernel(const __grid_constant__ Mat1D<P, Q, T> m, const BatchMesh<T>* __restrict__ meshes,
+                        const int2* __restrict__ tiles, int64_t n_tiles) {
+  using L = Mass3D<P, Q>;
+  extern __shared__ __align__(16) unsigned char smem_bytes[];
+  T* sa = reinterpret_cast<T*>(smem_bytes);
+  T* sb = sa + NCB * L::SA;
+  double dsum = 0.0;
+  for (int64_t g = blockIdx.x; g < n_tiles; g += gridDim.x) {
+    const int2 tm = tiles[g];
+    const BatchMesh<T> mm = meshes[tm.x];
+    mass3d_tile<P, Q, T, ApplyPlain, NCB>(m, sa, sb, mm.offs, mm.qd, mm.u, mm.v, nullptr, mm.num_elem, mm.comp_run,
+                                          mm.comp_stride, ApplyPlain{}, tm.y, dsum);
+  }
+}
+
+template <int P, int Q, class T>
+__global__ void __launch_bounds__(Mass2D<P, Q>::NT)
+    mass2d_batch_kernel(const __grid_constant__ Mat1D<P, Q, T> m, const BatchMesh<T>* __restrict__ meshes,
+                        const int2* __restrict__ tiles, int64_t n_tiles) {
+  using L = Mass2D<P, Q>;
+  extern __shared__ __align__(16) unsigned char smem_bytes[];
+  T* s1 = reinterpret_cast<T*>(smem_bytes);
+  T* s3 = s1 + L::S1;
+  double dsum = 0.0;
+  for (int64_t g = blockIdx.x; g < n_tiles; g += gridDim.x) {
+    const int2 tm = tiles[g];
+    const BatchMesh<T> mm = meshes[tm.x];
+    mass2d_tile<P, Q, T, ApplyPlain>(m, s1, s3, mm.offs, mm.qd, mm.u, mm.v, nullptr, mm.num_elem, mm.comp_run,
+                                     mm.comp_stride, ApplyPlain{}, tm.y, dsum);
+  }
+}
+
+template <int P, int Q, class T>
+__global__ void __launch_bounds__(128)
+    mass1d_batch_kernel(const __grid_constant__ Mat1D<P, Q, T> m, const BatchMesh<T>* __restrict__ meshes,
+                        const int2* __restrict__ tiles, int64_t n_tiles) {
+  double dsum = 0.0;
+  for (int64_t g = blockIdx.x; g < n_tiles; g += gridDim.x) {
+    const int2 tm = tiles[g];
+    const BatchMesh<T> mm = meshes[tm.x];
+    const int64_t eg = int64_t(tm.y) * 128 + threadIdx.x;
+    if (eg < mm.num_elem)
+      mass1d_element<P, Q, T, ApplyPlain>(m, mm.offs, mm.qd, mm.u, mm.v, nullptr, mm.num_elem, mm.comp_run,
+                                          mm.comp_stride, ApplyPlain{}, tm.y, int(threadIdx.x), eg, dsum);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+template <int P, int Q, class T>
+Mat1D<P, Q, T> batch_mat(const BasisData& b) {
+  Mat1D<P, Q, T> m;
+  for (int i = 0; i < Q * P; ++i) m.B[i] = T(b.interp[i]), m.G[i] = T(b.grad[i]);
+  for (int i = 0; i < Q; ++i) m.W[i] = T(b.q_weight[i]);
+  return m;
+}
+
+struct BatchClass;
+// Launch a class's kernel with `grid` CTAs (0: the occupancy-limited
+// persistent grid); returns the grid used.
+using ClassLauncher = unsigned (*)(const BatchClass&, const void* meshes, unsigned grid, cudaStream_t);
+
+struct BatchClass {
+  int dim = 0, P = 0, Q = 0, comp_run = 0, ncb = 1;
+  BasisData basis;
+  std::vector<int> members;  // indices into the batch
+  DevBuf<int2> tiles;
+  int64_t n_tiles = 0;
+  int64_t dofs = 0;        // sum of l_size (all components)
+  int schedule = 0;        // 0: one CTA per tile, 1: persistent
+  ClassLauncher launch = nullptr;
+};
+
+constexpr int kBatchMaxStreams = 4;
+
+// Resident CTAs per SM a 3D batch kernel asks for (a register cap): up to 4
+// for P <= 5 (3 with three components batched), 2 for P = 6, 1 above, and
+// no more than leave 56 registers a thread (72 with three components, 80 at
+// P = 6).
+constexpr int batch_min_blocks(int P, int threads, int ncb) {
+  const int cap = P > 6 ? 1 : P == 6 ? 2 : ncb == 3 ? 3 : 4;
+  const int regs = P == 6 ? 80 : ncb == 3 ? 72 : 56;
+  for (int b = cap; b > 1; --b)
+    if (b * threads <= 2048 && 65536 / (b * threads) >= regs) return b;
+  return 1;
+}
+
+template <int P, int Q, class T, int NCB>
+unsigned launch_batch3(const BatchClass& c, const void* meshes, unsigned grid, cudaStream_t s) {
+  using L = Mass3D<P, Q>;
+  constexpr int smem = NCB * (L::SA + L::SB) * int(sizeof(T));
+  constexpr int minb = batch_min_blocks(P, L::NT, NCB);
+  const auto kern = mass3d_batch_kernel<P, Q, minb, T, NCB>;
+  static std::atomic<uint64_t> smem_set{0};
+  set_smem(kern, smem, smem_set);
+  if (grid == 0) grid = unsigned(std::min<int64_t>(resident_ctas(reinterpret_cast<const void*>(kern), L::NT, smem),
+                                                   c.n_tiles));
+  kern<<<grid, L::NT, smem, s>>>(batch_mat<P, Q, T>(c.basis), static_cast<const BatchMesh<T>*>(meshes),
+                                 c.tiles.get(), c.n_tiles);
+  FEM_LAUNCH_CHECK();
+  return grid;
+}
+
+template <int P, int Q, class T>
+unsigned launch_batch2(const BatchClass& c, const void* meshes, unsigned grid, cudaStream_t s) {
+  using L = Mass2D<P, Q>;
+  constexpr int smem = (L::S1 + L::S3) * int(sizeof(T));
+  const auto kern = mass2d_batch_kernel<P, Q, T>;
+  static std::atomic<uint64_t> smem_set{0};
+  set_smem(kern, smem, smem_set);
+  if (grid == 0) grid = unsigned(std::min<int64_t>(resident_ctas(reinterpret_cast<const void*>(kern), L::NT, smem),
+                                                   c.n_tiles));
+  kern<<<grid, L::NT, smem, s>>>(batch_mat<P, Q, T>(c.basis), static_cast<const BatchMesh<T>*>(meshes),
+                                 c.tiles.get(), c.n_tiles);
+  FEM_LAUNCH_CHECK();
+  return grid;
+}
+
+template <int P, int Q, class T>
+unsigned launch_batch1(const BatchClass& c, const void* meshes, unsigned grid, cudaStream_t s) {
+  const auto kern = mass1d_batch_kernel<P, Q, T>;
+  if (grid == 0)
+    grid = unsigned(std::min<int64_t>(resident_ctas(reinterpret_cast<const void*>(kern), 128, 0), c.n_tiles));
+  kern<<<grid, 128, 0, s>>>(batch_mat<P, Q, T>(c.basis), static_cast<const BatchMesh<T>*>(meshes), c.tiles.get(),
+                            c.n_tiles);
+  FEM_LAUNCH_CHECK();
+  return grid;
+}
+
+constexpr int kBatchMinP = 2, kBatchMaxP = 8, kBatchQSpan = 3;
+
+// [dim-1][P][Q-P][ncb 1 or 3][T: 0 double, 1 float]
+struct BatchDispatch {
+  ClassLauncher fn[3][kBatchMaxP + 1][kBatchQSpan][2][2] = {};
+};
+
+template <int P, int DQ>
+struct BatchTable {
+  static void fill(BatchDispatch& d) {
+    constexpr int Q = P + DQ;
+    d.fn[0][P][DQ][0][0] = launch_batch1<P, Q, double>;
+    d.fn[0][P][DQ][0][1] = launch_batch1<P, Q, float>;
+    d.fn[1][P][DQ][0][0] = launch_batch2<P, Q, double>;
+    d.fn[1][P][DQ][0][1] = launch_batch2<P, Q, float>;
+    d.fn[2][P][DQ][0][0] = launch_batch3<P, Q, double, 1>;
+    d.fn[2][P][DQ][0][1] = launch_batch3<P, Q, float, 1>;
+    constexpr int smem8 = (Mass3D<P, Q>::SA + Mass3D<P, Q>::SB) * 8;
+    if constexpr (P <= 5 && 3 * smem8 <= kMaxSmemPerCta) d.fn[2][P][DQ][1][0] = launch_batch3<P, Q, double, 3>;
+    if constexpr (P <= 5 && 3 * smem8 / 2 <= kMaxSmemPerCta) d.fn[2][P][DQ][1][1] = launch_batch3<P, Q, float, 3>;
+    if constexpr (DQ + 1 < kBatchQSpan)
+      BatchTable<P, DQ + 1>::fill(d);
+    else if constexpr (P + 1 <= kBatchMaxP)
+      BatchTable<P + 1, 0>::fill(d);
+  }
+};
+
+const BatchDispatch& batch_dispatch() {
+  static const BatchDispatch d = [] {
+    BatchDispatch t;
+    BatchTable<kBatchMinP, 0>::fill(t);
+    return t;
+  }();
+  return d;
+}
+
+struct BatchPlan {
+  int device = 0;
+  int precision = 0;  // FEM_B200_PRECISION_FP64 / _FP32
+  std::vector<MassPlan*> ops;
+  std::vector<BatchClass> classes;
+  DevBuf<unsigned char> meshes;  // BatchMesh<T>[ops.size()]
+  std::vector<unsigned char> meshes_host;
+  bool bound = false;
+  int64_t max_l_size = 0;
+  cudaStream_t streams[kBatchMaxStreams] = {};
+  cudaEvent_t fork = nullptr, join[kBatchMaxStreams] = {};
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int graph_kernels = 0;
+
+  ~BatchPlan() {
+    int prev = -1;
+    (void)cudaGetDevice(&prev);
+    (void)cudaSetDevice(device);
+    if (exec) (void)cudaGraphExecDestroy(exec);
+    if (graph) (void)cudaGraphDestroy(graph);
+    for (auto& st : streams)
+      if (st) (void)cudaStreamDestroy(st);
+    for (auto& ev : join)
+      if (ev) (void)cudaEventDestroy(ev);
+    if (fork) (void)cudaEventDestroy(fork);
+    if (prev >= 0) (void)cudaSetDevice(prev);
+  }
+  size_t mesh_bytes() const { return precision == FEM_B200_PRECISION_FP32 ? sizeof(BatchMesh<float>) : sizeof(BatchMesh<double>); }
+  void drop_graph() {
+    if (exec) (void)cudaGraphExecDestroy(exec);
+    if (graph) (void)cudaGraphDestroy(graph);
+    exec = nullptr, graph = nullptr;
+  }
+};
+
+// Every v_i zeroed, then every class (the heaviest first, round-robin over
+// the streams, which fork from and join into s0).
+void enqueue_batch(BatchPlan& b, cudaStream_t s0, bool fork) {
+  const unsigned ops = unsigned(b.ops.size());
+  const unsigned zx = unsigned(std::max<int64_t>(1, std::min<int64_t>(64, (b.max_l_size + 2047) / 2048)));
+  if (b.precision == FEM_B200_PRECISION_FP32)
+    batch_zero_kernel<float><<<dim3(zx, ops), 256, 0, s0>>>(reinterpret_cast<const BatchMesh<float>*>(b.meshes.get()));
+  else
+    batch_zero_kernel<double><<<dim3(zx, ops), 256, 0, s0>>>(
+        reinterpret_cast<const BatchMesh<double>*>(b.meshes.get()));
+  FEM_LAUNCH_CHECK();
+  const int ns = fork ? int(std::min<size_t>(kBatchMaxStreams, b.classes.size())) : 1;
+  if (ns > 1) {
+    FEM_CUDA_CHECK(cudaEventRecord(b.fork, s0));
+    for (int i = 1; i < ns; ++i) FEM_CUDA_CHECK(cudaStreamWaitEvent(b.streams[i], b.fork, 0));
+  }
+  for (size_t c = 0; c < b.classes.size(); ++c) {
+    const BatchClass& cl = b.classes[c];
+    cudaStream_t s = (ns > 1 && c % ns) ? b.streams[c % ns] : s0;
+    cl.launch(cl, b.meshes.get(), cl.schedule == 0 ? unsigned(cl.n_tiles) : 0u, s);
+  }
+  if (ns > 1) {
+    for (int i = 1; i < ns; ++i) {
+      FEM_CUDA_CHECK(cudaEventRecord(b.join[i], b.streams[i]));
+      FEM_CUDA_CHECK(cudaStreamWaitEvent(s0, b.join[i], 0));
+    }
+  }
+}
+
+void capture_batch(BatchPlan& b) {
+  b.drop_graph();
+  cudaStream_t s0 = b.streams[0];
+  FEM_CUDA_CHECK(cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal));
+  try {
+    enqueue_batch(b, s0, true);
+  } catch (...) {
+    cudaGraph_t g = nullptr;
+    (void)cudaStreamEndCapture(s0, &g);
+    if (g) (void)cudaGraphDestroy(g);
+    throw;
+  }
+  FEM_CUDA_CHECK(cudaStreamEndCapture(s0, &b.graph));
+  FEM_CUDA_CHECK(cudaGraphInstantiate(&b.exec, b.graph, 0));
+  b.graph_kernels = 1 + int(b.classes.size());
+}
+
+template <class T>
+void write_descriptors(BatchPlan& b, const void* const* u, void* const* v) {
+  b.meshes_host.resize(b.ops.size() * sizeof(BatchMesh<T>));
+  auto* d = reinterpret_cast<BatchMesh<T>*>(b.meshes_host.data());
+  for (size_t i = 0; i < b.ops.size(); ++i) {
+    const MassPlan& p = *b.ops[i];
+    d[i].offs = p.offs_t.get();
+    d[i].qd = std::is_same<T, float>::value ? reinterpret_cast<const T*>(p.qd_t32.get())
+                                             : reinterpret_cast<const T*>(p.qd_t.get());
+    d[i].u = static_cast<const T*>(u[i]);
+    d[i].v = static_cast<T*>(v[i]);
+    d[i].l_size = p.l_size;
+    d[i].comp_stride = p.comp_stride;
+    d[i].num_elem = p.num_elem;
+    d[i].comp_run = p.comp_run;
+  }
+}
+
+}  // namespace fem_b200
+
+struct fem_b200_batch_s {
+  std::unique_ptr<fem_b200::BatchPlan> d;
+};
+
+using namespace fem_b200;
+
+extern "C" {
+
+int fem_b200_batch_create(const fem_b200_mass* ops, int num_ops, int precision, fem_b200_batch* out) {
+  return guarded([&] {
+    require(out != nullptr, "batch create: NULL output handle");
+    require(ops != nullptr && num_ops >= 1 && num_ops <= 65535, "batch create: 1..65535 operators");
+    require(precision == FEM_B200_PRECISION_FP64 || precision == FEM_B200_PRECISION_FP32,
+            "batch create: unknown precision");
+    auto b = std::make_unique<BatchPlan>();
+    b->precision = precision;
+    for (int i = 0; i < num_ops; ++i) {
+      require(ops[i] && ops[i]->d, "batch create: NULL operator");
+      b->ops.push_back(ops[i]->d.get());
+    }
+    b->device = b->ops[0]->device;
+    DeviceGuard g(b->device);
+    const BatchDispatch& disp = batch_dispatch();
+    const int ti = precision == FEM_B200_PRECISION_FP32 ? 1 : 0;
+    std::map<std::tuple<int, int, int, int, std::vector<double>>, int> index;
+    for (int i = 0; i < num_ops; ++i) {
+      MassPlan& p = *b->ops[i];
+      require(p.device == b->device, "batch create: every operator must be on the same device");
+      if (p.scatter_mode != FEM_B200_SCATTER_ATOMIC)
+        throw unsupported_error("batch create: operators with the deterministic scatter are not batched");
+      b->max_l_size = std::max<int64_t>(b->max_l_size, p.l_size);
+      if (ti == 1 && p.qd_t32.size() != p.qd_t.size()) {
+        p.qd_t32.alloc(p.qd_t.size());
+        batch_to_float_kernel<<<grid_for(int64_t(p.qd_t.size()), 256), 256>>>(int64_t(p.qd_t.size()), p.qd_t.get(),
+                                                                             p.qd_t32.get());
+        FEM_LAUNCH_CHECK();
+      }
+      const auto key = std::make_tuple(p.dim, p.P, p.Q, p.comp_run, p.basis.interp);
+      auto it = index.find(key);
+      if (it == index.end()) {
+        BatchClass c;
+        c.dim = p.dim, c.P = p.P, c.Q = p.Q, c.comp_run = p.comp_run;
+        c.basis = p.basis;
+        c.ncb = (p.dim == 3 && p.comp_run == 3 && p.P <= 5 && disp.fn[2][p.P][p.Q - p.P][1][ti]) ? 3 : 1;
+        c.launch = disp.fn[p.dim - 1][p.P][p.Q - p.P][c.ncb == 3 ? 1 : 0][ti];
+        require(c.launch != nullptr, "batch create: no batched kernel for this shape");
+        it = index.emplace(key, int(b->classes.size())).first;
+        b->classes.push_back(std::move(c));
+      }
+      BatchClass& c = b->classes[it->second];
+      c.members.push_back(i);
+      c.n_tiles += p.n_tiles;
+      c.dofs += p.l_size;
+    }
+    for (BatchClass& c : b->classes) {
+      require(c.n_tiles < (int64_t(1) << 31), "batch create: a class has more than 2^31 tiles");
+      std::vector<int2> t;
+      t.reserve(size_t(c.n_tiles));
+      for (int i : c.members)
+        for (int64_t k = 0; k < b->ops[i]->n_tiles; ++k) t.push_back(make_int2(i, int(k)));
+      c.tiles.alloc(t.size());
+      FEM_CUDA_CHECK(cudaMemcpy(c.tiles.get(), t.data(), t.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    }
+    // heaviest classes first, so the parallel branches start with the long kernels
+    std::stable_sort(b->classes.begin(), b->classes.end(),
+                     [](const BatchClass& x, const BatchClass& y) { return x.n_tiles > y.n_tiles; });
+    b->meshes.alloc(b->ops.size() * b->mesh_bytes());
+    for (auto& st : b->streams) FEM_CUDA_CHECK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    FEM_CUDA_CHECK(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+    for (auto& ev : b->join) FEM_CUDA_CHECK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    FEM_CUDA_CHECK(cudaDeviceSynchronize());
+    *out = new fem_b200_batch_s{std::move(b)};
+  });
+}
+
+int fem_b200_batch_bind(fem_b200_batch batch, const void* const* u, void* const* v, void* stream) {
+  return guarded([&] {
+    require(batch && batch->d, "batch bind: NULL handle");
+    BatchPlan& b = *batch->d;
+    require(u && v, "batch bind: NULL pointer arrays");
+    for (size_t i = 0; i < b.ops.size(); ++i) require(u[i] && v[i], "batch bind: NULL vector pointer");
+    DeviceGuard g(b.device);
+    if (b.precision == FEM_B200_PRECISION_FP32)
+      write_descriptors<float>(b, u, v);
+    else
+      write_descriptors<double>(b, u, v);
+    // pageable source: the copy is staged before the call returns
+    FEM_CUDA_CHECK(cudaMemcpyAsync(b.meshes.get(), b.meshes_host.data(), b.meshes_host.size(), cudaMemcpyHostToDevice,
+                                   as_stream(stream)));
+    b.bound = true;
+  });
+}
+
+int fem_b200_batch_apply(fem_b200_batch batch, int use_graph, void* stream) {
+  return guarded([&] {
+    require(batch && batch->d, "batch apply: NULL handle");
+    BatchPlan& b = *batch->d;
+    require(b.bound, "batch apply: bind the vectors first (fem_b200_batch_bind)");
+    DeviceGuard g(b.device);
+    cudaStream_t s = as_stream(stream);
+    if (!use_graph) {
+      enqueue_batch(b, s, false);
+      return;
+    }
+    if (!b.exec) {
+      // the kernels' attributes are set by one direct pass before the capture
+      enqueue_batch(b, s, false);
+      FEM_CUDA_CHECK(cudaStreamSynchronize(s));
+      capture_batch(b);
+    }
+    FEM_CUDA_CHECK(cudaGraphLaunch(b.exec, s));
+  });
+}
+
+int fem_b200_batch_autotune(fem_b200_batch batch, int reps, void* stream) {
+  return guarded([&] {
+    require(batch && batch->d, "batch autotune: NULL handle");
+    BatchPlan& b = *batch->d;
+    require(b.bound, "batch autotune: bind the vectors first (fem_b200_batch_bind)");
+    require(reps >= 1, "batch autotune: reps must be positive");
+    DeviceGuard g(b.device);
+    cudaStream_t s = as_stream(stream);
+    enqueue_batch(b, s, false);  // v zeroed; attributes set
+    cudaEvent_t e0, e1;
+    FEM_CUDA_CHECK(cudaEventCreate(&e0));
+    FEM_CUDA_CHECK(cudaEventCreate(&e1));
+    try {
+      for (BatchClass& c : b.classes) {
+        float best = 0.0f;
+        for (int sched = 0; sched < 2; ++sched) {
+          c.launch(c, b.meshes.get(), sched == 0 ? unsigned(c.n_tiles) : 0u, s);  // warm-up
+          FEM_CUDA_CHECK(cudaEventRecord(e0, s));
+          for (int r = 0; r < reps; ++r) c.launch(c, b.meshes.get(), sched == 0 ? unsigned(c.n_tiles) : 0u, s);
+          FEM_CUDA_CHECK(cudaEventRecord(e1, s));
+          FEM_CUDA_CHECK(cudaEventSynchronize(e1));
+          float ms = 0.0f;
+          FEM_CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+          if (sched == 0 || ms < best) best = ms, c.schedule = sched;
+        }
+      }
+    } catch (...) {
+      (void)cudaEventDestroy(e0);
+      (void)cudaEventDestroy(e1);
+      throw;
+    }
+    (void)cudaEventDestroy(e0);
+    (void)cudaEventDestroy(e1);
+    // the timing runs accumulated into v; leave the v_i = M_i u_i
+    enqueue_batch(b, s, false);
+    FEM_CUDA_CHECK(cudaStreamSynchronize(s));
+    b.drop_graph();
+  });
+}
+
+int fem_b200_batch_info(fem_b200_batch batch, int* num_classes, int64_t* total_tiles, int64_t* total_dofs,
+                        int* graph_kernels, int* persistent_classes) {
+  return guarded([&] {
+    require(batch && batch->d, "batch info: NULL handle");
+    const BatchPlan& b = *batch->d;
+    int64_t tiles = 0, dofs = 0;
+    int pers = 0;
+    for (const BatchClass& c : b.classes) tiles += c.n_tiles, dofs += c.dofs, pers += c.schedule;
+    if (num_classes) *num_classes = int(b.classes.size());
+    if (total_tiles) *total_tiles = tiles;
+    if (total_dofs) *total_dofs = dofs;
+    if (graph_kernels) *graph_kernels = 1 + int(b.classes.size());
+    if (persistent_classes) *persistent_classes = pers;
+  });
+}
+
+int fem_b200_batch_destroy(fem_b200_batch batch) {
+  return guarded([&] { delete batch; });
+}
+
+}  // extern "C"

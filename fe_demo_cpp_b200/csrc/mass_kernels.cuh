@@ -101,6 +101,150 @@ struct Mass3D {
                                               : 2048 / NT);
 };
 
+// One 8-element tile of the 3D fused apply (the body of mass3d_apply_kernel and
+// of the batched kernels): sa / sb are the CTA's shared buffers A and B.
+template <int P, int Q, class T, class Ext, int NCB>
+__device__ __forceinline__ void mass3d_tile(const Mat1D<P, Q, T>& m, T* __restrict__ sa, T* __restrict__ sb,
+                                            const int* __restrict__ offs, const T* __restrict__ qd,
+                                            const T* __restrict__ u, T* __restrict__ v, T* __restrict__ ev,
+                                            int num_elem, int num_comp_run, int64_t comp_stride,
+                                            const Ext& ext, const int64_t tile, double& dsum) {
+  using L = Mass3D<P, Q>;
+  constexpr int E = L::E;
+  const int t = threadIdx.x, e = t % E, col = t / E;
+  const bool nodal = col < P * P;  // (px, py) = (col % P, col / P)
+  const bool mixed = col < P * Q;  // (px, qz) = (col % P, col / P)
+  const int64_t eg = tile * E + e;
+  const bool valid = eg < num_elem;
+  // Prefetch: this thread's qdata row (qy, qz) = (col % Q, col / Q), all qx.
+  T qv[Q];
+  {
+    const T* qt = qd + tile * (int64_t(L::NQ) * E) + col * E + e;
+#pragma unroll
+    for (int qx = 0; qx < Q; ++qx) qv[qx] = __ldg(qt + qx * (Q * Q * E));
+  }
+  int off[P];
+  if (nodal) {
+    const int* ot = offs + tile * (int64_t(L::ES) * E) + col * E + e;
+#pragma unroll
+    for (int pz = 0; pz < P; ++pz) off[pz] = __ldg(ot + pz * (P * P * E));
+  }
+
+  for (int k0 = 0; k0 < num_comp_run; k0 += NCB) {
+    if (nodal) {  // phase A
+      T x[NCB][P];
+#pragma unroll
+      for (int pz = 0; pz < P; ++pz) {
+        T sc = T(1);
+        // the solver's diagonal is the same for every component of a node
+        if constexpr (Ext::kScale) sc = __ldg(ext.scale + off[pz]);
+#pragma unroll
+        for (int c = 0; c < NCB; ++c) {
+          x[c][pz] = __ldg(u + off[pz] + (k0 + c) * comp_stride);
+          if constexpr (Ext::kScale) x[c][pz] *= sc;
+        }
+      }
+      const int px = col % P, py = col / P;
+#pragma unroll
+      for (int c = 0; c < NCB; ++c) {
+#pragma unroll
+        for (int qz = 0; qz < Q; ++qz) {
+          T s = T(0);
+#pragma unroll
+          for (int pz = 0; pz < P; ++pz) s += m.B[qz * P + pz] * x[c][pz];
+          sa[c * L::SA + py * L::PS1 + (qz * P + px) * E + e] = s;
+        }
+      }
+    }
+    __syncthreads();
+    if (mixed) {  // phase B
+      const int px = col % P, qz = col / P;
+#pragma unroll
+      for (int c = 0; c < NCB; ++c) {
+        T y[P];
+#pragma unroll
+        for (int py = 0; py < P; ++py) y[py] = sa[c * L::SA + py * L::PS1 + col * E + e];
+#pragma unroll
+        for (int qy = 0; qy < Q; ++qy) {
+          T s = T(0);
+#pragma unroll
+          for (int py = 0; py < P; ++py) s += m.B[qy * P + py] * y[py];
+          sb[c * L::SB + px * L::PS2 + (qz * Q + qy) * E + e] = s;
+        }
+      }
+    }
+    __syncthreads();
+    {  // phase C: x, pointwise mass, x^T
+      const int qy = col % Q, qz = col / Q;
+#pragma unroll
+      for (int c = 0; c < NCB; ++c) {
+        T w[P];
+#pragma unroll
+        for (int px = 0; px < P; ++px) w[px] = sb[c * L::SB + px * L::PS2 + col * E + e];
+        T r[Q];
+#pragma unroll
+        for (int qx = 0; qx < Q; ++qx) {
+          T s = T(0);
+#pragma unroll
+          for (int px = 0; px < P; ++px) s += m.B[qx * P + px] * w[px];
+          r[qx] = qv[qx] * s;
+          if constexpr (Ext::kDot) dsum += double(r[qx]) * double(s);
+        }
+#pragma unroll
+        for (int px = 0; px < P; ++px) {
+          T s = T(0);
+#pragma unroll
+          for (int qx = 0; qx < Q; ++qx) s += m.B[qx * P + px] * r[qx];
+          sa[c * L::SA + qy * L::PS3 + (qz * P + px) * E + e] = s;
+        }
+      }
+    }
+    __syncthreads();
+    if (mixed) {  // phase F: y^T
+      const int px = col % P, qz = col / P;
+#pragma unroll
+      for (int c = 0; c < NCB; ++c) {
+        T y[Q];
+#pragma unroll
+        for (int qy = 0; qy < Q; ++qy) y[qy] = sa[c * L::SA + qy * L::PS3 + col * E + e];
+#pragma unroll
+        for (int py = 0; py < P; ++py) {
+          T s = T(0);
+#pragma unroll
+          for (int qy = 0; qy < Q; ++qy) s += m.B[qy * P + py] * y[qy];
+          sb[c * L::SB + qz * L::PS4 + (py * P + px) * E + e] = s;
+        }
+      }
+    }
+    __syncthreads();
+    if (nodal) {  // phase G: z^T and the scatter
+#pragma unroll
+      for (int c = 0; c < NCB; ++c) {
+        T z[Q];
+#pragma unroll
+        for (int qz = 0; qz < Q; ++qz) z[qz] = sb[c * L::SB + qz * L::PS4 + col * E + e];
+        const int64_t ks = (k0 + c) * comp_stride;
+#pragma unroll
+        for (int pz = 0; pz < P; ++pz) {
+          T s = T(0);
+#pragma unroll
+          for (int qz = 0; qz < Q; ++qz) s += m.B[qz * P + pz] * z[qz];
+          if (valid) {
+            if (ev)
+              ev[(int64_t(k0 + c) * L::ES + pz * P * P + col) * num_elem + eg] = s;
+            else
+              atomicAdd(v + off[pz] + ks, s);
+          }
+        }
+      }
+    }
+    // The next components' phase A writes buffer A, whose last readers
+    // (phase F) finished before the barrier above; their phase B writes
+    // buffer B only after the next barrier, which every phase-G reader has
+    // passed.  The same holds between one tile and the next.
+  }
+}
+
 // num_comp_run components are processed (1 for the reference apply_mass,
 // which only touches component 0); component k reads/writes at + k*comp_stride.
 // ev == nullptr: atomic scatter-add into v.  ev != nullptr: the element
@@ -123,152 +267,21 @@ __global__ void __launch_bounds__(Mass3D<P, Q>::NT, MINB) mass3d_apply_kernel(
   extern __shared__ __align__(16) unsigned char smem_bytes[];
   T* sa = reinterpret_cast<T*>(smem_bytes);
   T* sb = sa + NCB * L::SA;
-  const int t = threadIdx.x, e = t % E, col = t / E;
-  const bool nodal = col < P * P;  // (px, py) = (col % P, col / P)
-  const bool mixed = col < P * Q;  // (px, qz) = (col % P, col / P)
   if constexpr (Ext::kDot) {
     if (ext.st->done) return;  // uniform: the solve has stopped
   }
   double dsum = 0.0;
 
-  auto tile_body = [&](const int64_t tile) {
-    const int64_t eg = tile * E + e;
-    const bool valid = eg < num_elem;
-    // Prefetch: this thread's qdata row (qy, qz) = (col % Q, col / Q), all qx.
-    T qv[Q];
-    {
-      const T* qt = qd + tile * (int64_t(L::NQ) * E) + col * E + e;
-#pragma unroll
-      for (int qx = 0; qx < Q; ++qx) qv[qx] = __ldg(qt + qx * (Q * Q * E));
-    }
-    int off[P];
-    if (nodal) {
-      const int* ot = offs + tile * (int64_t(L::ES) * E) + col * E + e;
-#pragma unroll
-      for (int pz = 0; pz < P; ++pz) off[pz] = __ldg(ot + pz * (P * P * E));
-    }
-
-    for (int k0 = 0; k0 < num_comp_run; k0 += NCB) {
-      if (nodal) {  // phase A
-        T x[NCB][P];
-#pragma unroll
-        for (int pz = 0; pz < P; ++pz) {
-          T sc = T(1);
-          // the solver's diagonal is the same for every component of a node
-          if constexpr (Ext::kScale) sc = __ldg(ext.scale + off[pz]);
-#pragma unroll
-          for (int c = 0; c < NCB; ++c) {
-            x[c][pz] = __ldg(u + off[pz] + (k0 + c) * comp_stride);
-            if constexpr (Ext::kScale) x[c][pz] *= sc;
-          }
-        }
-        const int px = col % P, py = col / P;
-#pragma unroll
-        for (int c = 0; c < NCB; ++c) {
-#pragma unroll
-          for (int qz = 0; qz < Q; ++qz) {
-            T s = T(0);
-#pragma unroll
-            for (int pz = 0; pz < P; ++pz) s += m.B[qz * P + pz] * x[c][pz];
-            sa[c * L::SA + py * L::PS1 + (qz * P + px) * E + e] = s;
-          }
-        }
-      }
-      __syncthreads();
-      if (mixed) {  // phase B
-        const int px = col % P, qz = col / P;
-#pragma unroll
-        for (int c = 0; c < NCB; ++c) {
-          T y[P];
-#pragma unroll
-          for (int py = 0; py < P; ++py) y[py] = sa[c * L::SA + py * L::PS1 + col * E + e];
-#pragma unroll
-          for (int qy = 0; qy < Q; ++qy) {
-            T s = T(0);
-#pragma unroll
-            for (int py = 0; py < P; ++py) s += m.B[qy * P + py] * y[py];
-            sb[c * L::SB + px * L::PS2 + (qz * Q + qy) * E + e] = s;
-          }
-        }
-      }
-      __syncthreads();
-      {  // phase C: x, pointwise mass, x^T
-        const int qy = col % Q, qz = col / Q;
-#pragma unroll
-        for (int c = 0; c < NCB; ++c) {
-          T w[P];
-#pragma unroll
-          for (int px = 0; px < P; ++px) w[px] = sb[c * L::SB + px * L::PS2 + col * E + e];
-          T r[Q];
-#pragma unroll
-          for (int qx = 0; qx < Q; ++qx) {
-            T s = T(0);
-#pragma unroll
-            for (int px = 0; px < P; ++px) s += m.B[qx * P + px] * w[px];
-            r[qx] = qv[qx] * s;
-            if constexpr (Ext::kDot) dsum += double(r[qx]) * double(s);
-          }
-#pragma unroll
-          for (int px = 0; px < P; ++px) {
-            T s = T(0);
-#pragma unroll
-            for (int qx = 0; qx < Q; ++qx) s += m.B[qx * P + px] * r[qx];
-            sa[c * L::SA + qy * L::PS3 + (qz * P + px) * E + e] = s;
-          }
-        }
-      }
-      __syncthreads();
-      if (mixed) {  // phase F: y^T
-        const int px = col % P, qz = col / P;
-#pragma unroll
-        for (int c = 0; c < NCB; ++c) {
-          T y[Q];
-#pragma unroll
-          for (int qy = 0; qy < Q; ++qy) y[qy] = sa[c * L::SA + qy * L::PS3 + col * E + e];
-#pragma unroll
-          for (int py = 0; py < P; ++py) {
-            T s = T(0);
-#pragma unroll
-            for (int qy = 0; qy < Q; ++qy) s += m.B[qy * P + py] * y[qy];
-            sb[c * L::SB + qz * L::PS4 + (py * P + px) * E + e] = s;
-          }
-        }
-      }
-      __syncthreads();
-      if (nodal) {  // phase G: z^T and the scatter
-#pragma unroll
-        for (int c = 0; c < NCB; ++c) {
-          T z[Q];
-#pragma unroll
-          for (int qz = 0; qz < Q; ++qz) z[qz] = sb[c * L::SB + qz * L::PS4 + col * E + e];
-          const int64_t ks = (k0 + c) * comp_stride;
-#pragma unroll
-          for (int pz = 0; pz < P; ++pz) {
-            T s = T(0);
-#pragma unroll
-            for (int qz = 0; qz < Q; ++qz) s += m.B[qz * P + pz] * z[qz];
-            if (valid) {
-              if (ev)
-                ev[(int64_t(k0 + c) * L::ES + pz * P * P + col) * num_elem + eg] = s;
-              else
-                atomicAdd(v + off[pz] + ks, s);
-            }
-          }
-        }
-      }
-      // The next components' phase A writes buffer A, whose last readers
-      // (phase F) finished before the barrier above; their phase B writes
-      // buffer B only after the next barrier, which every phase-G reader has
-      // passed.  The same holds between one tile and the next.
-    }
-  };
   if constexpr (Ext::kDot) {  // persistent: one reduction per CTA
     const int64_t n_tiles = (int64_t(num_elem) + E - 1) / E;
-    for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) tile_body(tile);
+    for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x)
+      mass3d_tile<P, Q, T, Ext, NCB>(m, sa, sb, offs, qd, u, v, ev, num_elem, num_comp_run, comp_stride, ext, tile,
+                                     dsum);
     double dv[1] = {dsum};
     grid_sum<1>(dv, ext.part, &ext.st->ticket, [&](const double* tot) { cg_after_apply(ext.st, tot[0]); });
   } else {
-    tile_body(blockIdx.x);
+    mass3d_tile<P, Q, T, Ext, NCB>(m, sa, sb, offs, qd, u, v, ev, num_elem, num_comp_run, comp_stride, ext,
+                                   blockIdx.x, dsum);
   }
 }
 
@@ -405,6 +418,92 @@ struct Mass2D {
   static constexpr int ES = P * P, NQ = Q * Q;
 };
 
+// One 32-element tile of the 2D fused apply: s1 / s3 the CTA's shared buffers.
+template <int P, int Q, class T, class Ext>
+__device__ __forceinline__ void mass2d_tile(const Mat1D<P, Q, T>& m, T* __restrict__ s1, T* __restrict__ s3,
+                                            const int* __restrict__ offs, const T* __restrict__ qd,
+                                            const T* __restrict__ u, T* __restrict__ v, T* __restrict__ ev,
+                                            int num_elem, int num_comp_run, int64_t comp_stride,
+                                            const Ext& ext, const int64_t tile, double& dsum) {
+  using L = Mass2D<P, Q>;
+  constexpr int E = L::E;
+  const int t = threadIdx.x, e = t % E, col = t / E;
+  const bool nodal = col < P;
+  const int64_t eg = tile * E + e;
+  const bool valid = eg < num_elem;
+  T qv[Q];
+  {
+    const T* qt = qd + tile * (int64_t(L::NQ) * E) + col * E + e;
+#pragma unroll
+    for (int qx = 0; qx < Q; ++qx) qv[qx] = __ldg(qt + qx * (Q * E));
+  }
+  int off[P];
+  if (nodal) {
+    const int* ot = offs + tile * (int64_t(L::ES) * E) + col * E + e;
+#pragma unroll
+    for (int py = 0; py < P; ++py) off[py] = __ldg(ot + py * (P * E));
+  }
+  for (int k = 0; k < num_comp_run; ++k) {
+    const int64_t ks = k * comp_stride;
+    if (nodal) {
+      T x[P];
+#pragma unroll
+      for (int py = 0; py < P; ++py) {
+        x[py] = __ldg(u + off[py] + ks);
+        if constexpr (Ext::kScale) x[py] *= __ldg(ext.scale + off[py]);
+      }
+#pragma unroll
+      for (int qy = 0; qy < Q; ++qy) {
+        T s = T(0);
+#pragma unroll
+        for (int py = 0; py < P; ++py) s += m.B[qy * P + py] * x[py];
+        s1[(col * Q + qy) * E + e] = s;
+      }
+    }
+    __syncthreads();
+    {
+      T w[P];
+#pragma unroll
+      for (int px = 0; px < P; ++px) w[px] = s1[(px * Q + col) * E + e];
+      T r[Q];
+#pragma unroll
+      for (int qx = 0; qx < Q; ++qx) {
+        T s = T(0);
+#pragma unroll
+        for (int px = 0; px < P; ++px) s += m.B[qx * P + px] * w[px];
+        r[qx] = qv[qx] * s;
+        if constexpr (Ext::kDot) dsum += double(r[qx]) * double(s);
+      }
+#pragma unroll
+      for (int px = 0; px < P; ++px) {
+        T s = T(0);
+#pragma unroll
+        for (int qx = 0; qx < Q; ++qx) s += m.B[qx * P + px] * r[qx];
+        s3[(col * P + px) * E + e] = s;
+      }
+    }
+    __syncthreads();
+    if (nodal) {
+      T z[Q];
+#pragma unroll
+      for (int qy = 0; qy < Q; ++qy) z[qy] = s3[(qy * P + col) * E + e];
+#pragma unroll
+      for (int py = 0; py < P; ++py) {
+        T s = T(0);
+#pragma unroll
+        for (int qy = 0; qy < Q; ++qy) s += m.B[qy * P + py] * z[qy];
+        if (valid) {
+          if (ev)
+            ev[(int64_t(k) * L::ES + py * P + col) * num_elem + eg] = s;
+          else
+            atomicAdd(v + off[py] + ks, s);
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
 template <int P, int Q, class T = double, class Ext = ApplyPlain>
 __global__ void __launch_bounds__(Mass2D<P, Q>::NT) mass2d_apply_kernel(
     const __grid_constant__ Mat1D<P, Q, T> m, const int* __restrict__ offs, const T* __restrict__ qd,
@@ -415,94 +514,19 @@ __global__ void __launch_bounds__(Mass2D<P, Q>::NT) mass2d_apply_kernel(
   extern __shared__ __align__(16) unsigned char smem_bytes[];
   T* s1 = reinterpret_cast<T*>(smem_bytes);
   T* s3 = s1 + L::S1;
-  const int t = threadIdx.x, e = t % E, col = t / E;
-  const bool nodal = col < P;
   if constexpr (Ext::kDot) {
     if (ext.st->done) return;
   }
   double dsum = 0.0;
-  auto tile_body = [&](const int64_t tile) {
-    const int64_t eg = tile * E + e;
-    const bool valid = eg < num_elem;
-    T qv[Q];
-    {
-      const T* qt = qd + tile * (int64_t(L::NQ) * E) + col * E + e;
-#pragma unroll
-      for (int qx = 0; qx < Q; ++qx) qv[qx] = __ldg(qt + qx * (Q * E));
-    }
-    int off[P];
-    if (nodal) {
-      const int* ot = offs + tile * (int64_t(L::ES) * E) + col * E + e;
-#pragma unroll
-      for (int py = 0; py < P; ++py) off[py] = __ldg(ot + py * (P * E));
-    }
-    for (int k = 0; k < num_comp_run; ++k) {
-      const int64_t ks = k * comp_stride;
-      if (nodal) {
-        T x[P];
-#pragma unroll
-        for (int py = 0; py < P; ++py) {
-          x[py] = __ldg(u + off[py] + ks);
-          if constexpr (Ext::kScale) x[py] *= __ldg(ext.scale + off[py]);
-        }
-#pragma unroll
-        for (int qy = 0; qy < Q; ++qy) {
-          T s = T(0);
-#pragma unroll
-          for (int py = 0; py < P; ++py) s += m.B[qy * P + py] * x[py];
-          s1[(col * Q + qy) * E + e] = s;
-        }
-      }
-      __syncthreads();
-      {
-        T w[P];
-#pragma unroll
-        for (int px = 0; px < P; ++px) w[px] = s1[(px * Q + col) * E + e];
-        T r[Q];
-#pragma unroll
-        for (int qx = 0; qx < Q; ++qx) {
-          T s = T(0);
-#pragma unroll
-          for (int px = 0; px < P; ++px) s += m.B[qx * P + px] * w[px];
-          r[qx] = qv[qx] * s;
-          if constexpr (Ext::kDot) dsum += double(r[qx]) * double(s);
-        }
-#pragma unroll
-        for (int px = 0; px < P; ++px) {
-          T s = T(0);
-#pragma unroll
-          for (int qx = 0; qx < Q; ++qx) s += m.B[qx * P + px] * r[qx];
-          s3[(col * P + px) * E + e] = s;
-        }
-      }
-      __syncthreads();
-      if (nodal) {
-        T z[Q];
-#pragma unroll
-        for (int qy = 0; qy < Q; ++qy) z[qy] = s3[(qy * P + col) * E + e];
-#pragma unroll
-        for (int py = 0; py < P; ++py) {
-          T s = T(0);
-#pragma unroll
-          for (int qy = 0; qy < Q; ++qy) s += m.B[qy * P + py] * z[qy];
-          if (valid) {
-            if (ev)
-              ev[(int64_t(k) * L::ES + py * P + col) * num_elem + eg] = s;
-            else
-              atomicAdd(v + off[py] + ks, s);
-          }
-        }
-      }
-      __syncthreads();
-    }
-  };
   if constexpr (Ext::kDot) {  // persistent, one reduction per CTA
     const int64_t n_tiles = (int64_t(num_elem) + E - 1) / E;
-    for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) tile_body(tile);
+    for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x)
+      mass2d_tile<P, Q, T, Ext>(m, s1, s3, offs, qd, u, v, ev, num_elem, num_comp_run, comp_stride, ext, tile, dsum);
     double dv[1] = {dsum};
     grid_sum<1>(dv, ext.part, &ext.st->ticket, [&](const double* tot) { cg_after_apply(ext.st, tot[0]); });
   } else {
-    tile_body(blockIdx.x);
+    mass2d_tile<P, Q, T, Ext>(m, s1, s3, offs, qd, u, v, ev, num_elem, num_comp_run, comp_stride, ext, blockIdx.x,
+                              dsum);
   }
 }
 

@@ -67,6 +67,7 @@ extern "C" {
 typedef struct fem_b200_restriction_s *fem_b200_restriction;
 typedef struct fem_b200_basis_s *fem_b200_basis;
 typedef struct fem_b200_mass_s *fem_b200_mass;
+typedef struct fem_b200_batch_s *fem_b200_batch;
 
 /* Message of this thread's last failure ("" if none). */
 const char *fem_b200_last_error(void);
@@ -308,16 +309,20 @@ int fem_b200_mass_autotune(fem_b200_mass op, const double *u, int64_t n_u, doubl
  * (its survey verifies it against e_i^T M e_i on small meshes). */
 int fem_b200_mass_diagonal(fem_b200_mass op, double *diag, int64_t n, void *stream);
 
-/* Solve M u = f (device arrays, l_size) by Jacobi-preconditioned CG from u = 0.
+/* Solve M u = f (device arrays, l_size) by Jacobi-preconditioned CG from u = 0
+ * (Chronopoulos-Gear form: one grid reduction point per iteration, scalars kept
+ * on the device, the host checking convergence between batches of queued
+ * iterations; reductions in FP64, in a fixed order).
  *   FEM_B200_SOLVE_FP64     FP64 PCG to ||r|| <= rtol ||f|| (recursive residual);
  *   FEM_B200_SOLVE_FP32_IR  FP64 iterative refinement: r = f - M u in FP64, a
  *                           correction from FP32 PCG (FP32 qdata, vectors and
- *                           fused apply; FP64 dot products) on r / ||r|| to 1e-5,
- *                           until ||f - M u|| <= rtol ||f||.
+ *                           fused apply; FP64 reductions) on r / ||r||, each
+ *                           inner solve to what the target still needs (not
+ *                           below 5e-6), until ||f - M u|| <= rtol ||f||.
  * max_iter bounds the CG iterations (all inner ones for FP32_IR).  Outputs (any
  * may be NULL): total CG iterations, refinement steps, and the true FP64
- * relative residual ||f - M u|| / ||f|| (one extra FP64 apply).  Synchronises
- * the stream.  Plans of the reference apply_mass with num_comp > 1 are
+ * relative residual ||f - M u|| / ||f||.  Plans with the deterministic scatter
+ * reproduce every bit of u from run to run.  Synchronises the stream.  Plans of the reference apply_mass with num_comp > 1 are
  * singular (components 1.. are left out) and return FEM_B200_ERROR_UNSUPPORTED.
  * No reference counterpart (the reference has no solver). */
 #define FEM_B200_SOLVE_FP64 0
@@ -325,6 +330,36 @@ int fem_b200_mass_diagonal(fem_b200_mass op, double *diag, int64_t n, void *stre
 int fem_b200_mass_solve(fem_b200_mass op, const double *f, int64_t n_f, double *u, int64_t n_u, double rtol,
                         int max_iter, int precision, int *iterations, int *refinements, double *rel_residual,
                         void *stream);
+
+/* ---- batched apply over many meshes (no reference counterpart) ------------
+ * One batch = many mass operators (any dim, P, Q, num_comp; atomic scatter)
+ * applied together: v_i = M_i u_i for all i, as ONE captured CUDA graph
+ * (a kernel zeroing every v_i, then one kernel per class of equal dim, P, Q,
+ * components and basis over a device table of (mesh, tile) pairs, classes on
+ * parallel graph branches).  The operators must outlive the batch.
+ * Precision FEM_B200_PRECISION_FP32 applies FP32 u_i / v_i with FP32 qdata
+ * (converted once from each operator's FP64 qdata). */
+#define FEM_B200_PRECISION_FP64 0
+#define FEM_B200_PRECISION_FP32 1
+int fem_b200_batch_create(const fem_b200_mass *ops, int num_ops, int precision, fem_b200_batch *out);
+/* Device pointers u[i], v[i] (double or float per the batch's precision, each
+ * of operator i's l_size), written into the batch's device descriptor table
+ * in `stream` order; the captured graph reads them at launch, so rebinding
+ * needs no new capture. */
+int fem_b200_batch_bind(fem_b200_batch b, const void *const *u, void *const *v, void *stream);
+/* v_i = M_i u_i for every i.  use_graph != 0: launch the captured graph
+ * (captured on the first call, from streams of the batch's own); 0: the same
+ * kernels launched one by one into `stream`. */
+int fem_b200_batch_apply(fem_b200_batch b, int use_graph, void *stream);
+/* Time each class's schedules (one CTA per tile; a persistent grid of
+ * resident CTAs) over `reps` launches, keep the faster, and re-capture at
+ * the next graph apply.  Leaves v_i = M_i u_i.  Synchronises the stream. */
+int fem_b200_batch_autotune(fem_b200_batch b, int reps, void *stream);
+/* Any output may be NULL: classes, tiles, sum of l_size (DoFs), kernels per
+ * graph launch, classes on the persistent schedule. */
+int fem_b200_batch_info(fem_b200_batch b, int *num_classes, int64_t *total_tiles, int64_t *total_dofs,
+                        int *graph_kernels, int *persistent_classes);
+int fem_b200_batch_destroy(fem_b200_batch b);
 
 /* Synchronise `stream` and report a device-side failure of the plan's kernels
  * (a bounded wait that ran out) as FEM_B200_ERROR_CUDA.  fem_b200_mass_apply_host
