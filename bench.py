@@ -606,6 +606,88 @@ def run_batch(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# served mass solves: Poisson arrivals at swept rates; each request a 3D box
+# with elements log-uniform in [8^3, 64^3], P uniform in 2..6, num_comp 1 or 3,
+# f ~ U[-1,1], rtol 1e-10; admitted by a 120 GB device budget; mixed precision
+# against the plain FP64 path (extra lines)
+# ---------------------------------------------------------------------------
+def serve_requests(n, seed):
+    rng = np.random.default_rng([seed, 5])
+    out = []
+    for i in range(n):
+        side = int(round(float(np.exp(rng.uniform(np.log(8), np.log(64))))))
+        out.append(((side,) * 3, int(rng.integers(2, 7)), 1 if rng.random() < 0.5 else 3, 1000 + i))
+    return out
+
+
+def run_serve(args):
+    import threading
+    import torch
+    import fe_demo_cpp_b200 as fem
+    from fe_demo_cpp_b200.build import build
+    from fe_demo_cpp_b200.telemetry import ClockSampler
+
+    build()
+    torch.cuda.set_device(0)
+    rates = [float(r) for r in args.serve_rates.split(",")]
+    reqs = serve_requests(args.serve_requests, SEED)
+    budget = int(args.serve_budget_gb * (1 << 30))
+    sampler = ClockSampler(0).start()
+    lines = []
+    for prec in ("fp32_ir", "fp64"):
+        with fem.Server(slots=args.serve_slots, hbm_budget=budget) as srv:
+            # warm-up: one request of each order (kernel attributes, pool)
+            for Pw in range(2, 7):
+                srv.wait(srv.submit_box(3, (8, 8, 8), Pw, num_comp=3, seed=1, precision=prec))
+            for rate in rates:
+                rng = np.random.default_rng([SEED, int(rate)])
+                gaps = rng.exponential(1.0 / rate, len(reqs))
+                ids = [None] * len(reqs)
+
+                def client():
+                    t = time.perf_counter()
+                    for k, (shape, Pp, nc, seed) in enumerate(reqs):
+                        t += gaps[k]
+                        delay = t - time.perf_counter()
+                        if delay > 0:
+                            time.sleep(delay)
+                        ids[k] = srv.submit_box(3, shape, Pp, num_comp=nc, seed=seed, rtol=1e-10, precision=prec)
+                th = threading.Thread(target=client)
+                th.start()
+                res = []
+                for k in range(len(reqs)):
+                    while ids[k] is None:
+                        time.sleep(0.0005)
+                    res.append(srv.wait(ids[k]))
+                th.join()
+                st = srv.stats()
+                bad = [r for r in res if r["status"] != 0]
+                assert not bad, bad[0]["message"]
+                lat = sorted((r["t_end"] - r["t_submit"]) * 1e3 for r in res)
+                span = max(r["t_end"] for r in res) - min(r["t_submit"] for r in res)
+                lines.append({
+                    "serve": "mass_solve", "precision": prec, "rate_rps": rate, "requests": len(res),
+                    "metric": "solves/s", "value": len(res) / span, "unit": "solves/s",
+                    "p50_ms": lat[len(lat) // 2], "p99_ms": lat[min(len(lat) - 1, int(round(0.99 * (len(lat) - 1))))],
+                    "mean_queue_ms": float(np.mean([(r["t_start"] - r["t_submit"]) * 1e3 for r in res])),
+                    "mean_service_ms": float(np.mean([(r["t_end"] - r["t_start"]) * 1e3 for r in res])),
+                    "gdofs_solved_per_s": sum(r["dofs"] for r in res) / span / 1e9,
+                    "mean_dofs": float(np.mean([r["dofs"] for r in res])),
+                    "mean_iterations": float(np.mean([r["iterations"] for r in res])),
+                    "max_rel_residual": max(r["rel_residual"] for r in res),
+                    "bytes_peak": st["bytes_peak"],
+                    "config": {"slots": args.serve_slots, "budget_bytes": budget,
+                               "requests": "3D boxes, elements log-uniform in [8^3, 64^3] (cubes), P uniform 2..6, "
+                                           "Q=P+1, num_comp 1 or 3, f ~ U[-1,1], rtol 1e-10, Poisson arrivals",
+                               "mesh": "generated on the device per request; set-up (mesh, qdata, plan) inside "
+                                       "each request's latency"}})
+                print(json.dumps(lines[-1]), flush=True)
+    clocks = sampler.stop()
+    print(json.dumps({"serve": "clocks", "clocks": clocks}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -629,7 +711,14 @@ def main():
     ap.add_argument("--batch", action="store_true", help="512 uneven meshes in one graph, FP64 and FP32 (extra lines)")
     ap.add_argument("--batch-meshes", type=int, default=512)
     ap.add_argument("--batch-steps", type=int, default=20)
+    ap.add_argument("--serve", action="store_true", help="served solve stream at swept Poisson rates (extra lines)")
+    ap.add_argument("--serve-rates", default="50,200,1000,2000")
+    ap.add_argument("--serve-requests", type=int, default=64)
+    ap.add_argument("--serve-slots", type=int, default=8)
+    ap.add_argument("--serve-budget-gb", type=float, default=120.0)
     args = ap.parse_args()
+    if args.serve:
+        return run_serve(args)
     if args.batch:
         return run_batch(args)
     if args.sweep:

@@ -18,6 +18,7 @@ from .api import (  # noqa: F401
     QuadMode,
     Restriction,
     ScatterMode,
+    Server,
     check_offset_restriction,
     check_strided_restriction,
     gauss_legendre_quadrature,

@@ -12,7 +12,7 @@ import os
 PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG, "lib", "libfem_b200.so")
 
-SUCCESS, ERROR_ARGUMENT, ERROR_CUDA, ERROR_UNSUPPORTED = 0, 1, 2, 3
+SUCCESS, ERROR_ARGUMENT, ERROR_CUDA, ERROR_UNSUPPORTED, NOT_READY = 0, 1, 2, 3, 4
 
 _i, _i64, _p, _dp, _ip = C.c_int, C.c_int64, C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int)
 
@@ -70,6 +70,11 @@ SIGNATURES = {
     "fem_b200_batch_autotune": ([_p, _i, _p], _i),
     "fem_b200_batch_info": ([_p, _p, _p, _p, _p, _p], _i),
     "fem_b200_batch_destroy": ([_p], _i),
+    "fem_b200_server_create": ([_i, _i64, _p], _i),
+    "fem_b200_server_submit": ([_p, _p, _p], _i),
+    "fem_b200_server_wait": ([_p, _i64, C.c_double, _p], _i),
+    "fem_b200_server_stats": ([_p, _p, _p, _p, _p, _p, _p], _i),
+    "fem_b200_server_destroy": ([_p], _i),
     "fem_b200_mass_autotune": ([_p, _p, _i64, _p, _i64, _i, _p, _p, _p], _i),
 }
 
@@ -108,6 +113,8 @@ def check(rc: int) -> None:
         raise ValueError(msg)
     if rc == ERROR_UNSUPPORTED:
         raise FemUnsupported(msg)
+    if rc == NOT_READY:
+        raise TimeoutError("the request has not finished within the timeout")
     raise FemError(msg)
 
 

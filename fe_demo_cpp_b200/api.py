@@ -360,3 +360,95 @@ class Batch(_Handle):
              C.addressof(gk), C.addressof(pc))
         return {"classes": nc.value, "tiles": tiles.value, "dofs": dofs.value, "graph_kernels": gk.value,
                 "persistent_classes": pc.value}
+
+
+class _Request(C.Structure):
+    """fem_b200_request (include/fem_b200.h)."""
+    _fields_ = [("kind", C.c_int), ("dim", C.c_int), ("P", C.c_int), ("Q", C.c_int), ("num_comp", C.c_int),
+                ("shape", C.c_int * 3), ("perturb", C.c_double), ("seed", C.c_uint64),
+                ("num_elem", C.c_int), ("num_nodes", C.c_int), ("offsets", C.c_void_p), ("coords", C.c_void_p),
+                ("f", C.c_void_p), ("rtol", C.c_double), ("max_iter", C.c_int), ("precision", C.c_int),
+                ("scatter_mode", C.c_int), ("u_out", C.c_void_p), ("f_out", C.c_void_p)]
+
+
+class _Result(C.Structure):
+    """fem_b200_result (include/fem_b200.h)."""
+    _fields_ = [("status", C.c_int), ("iterations", C.c_int), ("refinements", C.c_int),
+                ("rel_residual", C.c_double), ("t_submit", C.c_double), ("t_start", C.c_double),
+                ("t_end", C.c_double), ("dofs", C.c_int64), ("device_bytes", C.c_int64),
+                ("message", C.c_char * 256)]
+
+
+class Server(_Handle):
+    """Served mass solves (fem_b200_server_*): requests admitted by a device-
+    memory budget into `slots` concurrent workers; see include/fem_b200.h."""
+    _destroy = "fem_b200_server_destroy"
+
+    def __init__(self, slots: int = 4, hbm_budget: int = 120 << 30):
+        super().__init__()
+        call("fem_b200_server_create", int(slots), int(hbm_budget), C.addressof(self.h))
+        self._keep = {}  # host arrays a queued request still reads or writes
+
+    def _submit(self, req, keep):
+        rid = C.c_int64(0)
+        call("fem_b200_server_submit", self.h, C.addressof(req), C.addressof(rid))
+        self._keep[rid.value] = keep
+        return rid.value
+
+    @staticmethod
+    def _common(req, dim, P, Q, num_comp, rtol, max_iter, precision, deterministic, u_out, f_out):
+        req.dim, req.P, req.Q, req.num_comp = int(dim), int(P), int(Q if Q is not None else P + 1), int(num_comp)
+        req.rtol, req.max_iter = float(rtol), int(max_iter)
+        req.precision = {"fp64": 0, "fp32_ir": 1}[precision]
+        req.scatter_mode = 1 if deterministic else 0
+        for name, a in (("u_out", u_out), ("f_out", f_out)):
+            if a is not None:
+                if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]):
+                    raise ValueError(f"{name} must be a contiguous float64 numpy array")
+                setattr(req, name, a.ctypes.data)
+
+    def submit_box(self, dim, shape, P, Q=None, num_comp=1, seed=0, perturb=0.1, rtol=1e-10, max_iter=2000,
+                   precision="fp32_ir", deterministic=False, u_out=None, f_out=None) -> int:
+        """A box [0,1]^dim of `shape` elements generated on the device, f ~ U[-1,1]."""
+        req = _Request()
+        req.kind = 0
+        self._common(req, dim, P, Q, num_comp, rtol, max_iter, precision, deterministic, u_out, f_out)
+        for d, n in enumerate(shape):
+            req.shape[d] = int(n)
+        req.perturb, req.seed = float(perturb), int(seed)
+        return self._submit(req, (u_out, f_out))
+
+    def submit_mesh(self, dim, P, offsets, coords, f, Q=None, num_comp=1, rtol=1e-10, max_iter=2000,
+                    precision="fp32_ir", deterministic=False, u_out=None) -> int:
+        """A mesh from host arrays: offsets [num_elem*P^dim] int32, coordinates
+        blocked [dim*num_nodes], f blocked [num_comp*num_nodes]."""
+        offsets = np.ascontiguousarray(offsets, dtype=np.int32)
+        coords = np.ascontiguousarray(coords, dtype=np.float64)
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        req = _Request()
+        req.kind = 1
+        self._common(req, dim, P, Q, num_comp, rtol, max_iter, precision, deterministic, u_out, None)
+        req.num_elem = offsets.size // (int(P) ** int(dim))
+        req.num_nodes = coords.size // int(dim)
+        if f.size != req.num_nodes * int(num_comp):
+            raise ValueError("submit_mesh: f must have num_comp * num_nodes entries")
+        req.offsets, req.coords, req.f = offsets.ctypes.data, coords.ctypes.data, f.ctypes.data
+        return self._submit(req, (offsets, coords, f, u_out))
+
+    def wait(self, rid: int, timeout=None) -> dict:
+        res = _Result()
+        call("fem_b200_server_wait", self.h, int(rid), -1.0 if timeout is None else float(timeout),
+             C.addressof(res))
+        self._keep.pop(rid, None)
+        return {"status": res.status, "iterations": res.iterations, "refinements": res.refinements,
+                "rel_residual": res.rel_residual, "t_submit": res.t_submit, "t_start": res.t_start,
+                "t_end": res.t_end, "dofs": res.dofs, "device_bytes": res.device_bytes,
+                "message": res.message.decode()}
+
+    def stats(self) -> dict:
+        sub, comp, pend, use, peak = (C.c_int64(0) for _ in range(5))
+        run = C.c_int(0)
+        call("fem_b200_server_stats", self.h, C.addressof(sub), C.addressof(comp), C.addressof(run),
+             C.addressof(pend), C.addressof(use), C.addressof(peak))
+        return {"submitted": sub.value, "completed": comp.value, "running": run.value, "pending": pend.value,
+                "bytes_in_use": use.value, "bytes_peak": peak.value}

@@ -228,6 +228,10 @@ std::string shape_str(int dim, int P, int Q) {
   return "dim=" + std::to_string(dim) + ", P=" + std::to_string(P) + ", Q=" + std::to_string(Q);
 }
 
+bool device_path_supported(int dim, int P, int Q) {
+  return fused_supported(dim, P, Q) && !(dim == 3 && build3d_smem(P, Q) > kMaxSmemPerCta);
+}
+
 }  // namespace fem_b200
 
 using namespace fem_b200;
@@ -342,28 +346,8 @@ int fem_b200_restriction_create_offset(int num_elem, int elem_size, int num_comp
             "elem_restriction_create: unknown scatter mode");
     const int64_t n_t = int64_t(num_elem) * elem_size;
     check_offset(num_elem, elem_size, num_comp, comp_stride, l_size, offsets, n_t);
-    auto d = std::make_shared<RestrictionData>();
-    d->device = current_device();
-    d->num_elem = num_elem, d->elem_size = elem_size, d->num_comp = num_comp;
-    d->comp_stride = comp_stride;
-    d->l_size = l_size;
-    d->e_size = int64_t(num_comp) * n_t;
-    d->scatter_mode = scatter_mode;
-    d->offsets.alloc(size_t(n_t));
-    FEM_CUDA_CHECK(cudaMemcpy(d->offsets.get(), offsets, n_t * sizeof(int), cudaMemcpyHostToDevice));
-    if (scatter_mode == FEM_B200_SCATTER_DETERMINISTIC) {
-      std::vector<int> lvi(static_cast<size_t>(l_size)), toff(static_cast<size_t>(l_size) + 1),
-          tidx(static_cast<size_t>(n_t));
-      const int n = transpose_map(num_elem, elem_size, l_size, offsets, lvi.data(), toff.data(), tidx.data());
-      d->num_nodes = n;
-      d->l_vec_indices.alloc(size_t(n));
-      d->t_offsets.alloc(size_t(n) + 1);
-      d->t_indices.alloc(size_t(n_t));
-      FEM_CUDA_CHECK(cudaMemcpy(d->l_vec_indices.get(), lvi.data(), n * sizeof(int), cudaMemcpyHostToDevice));
-      FEM_CUDA_CHECK(cudaMemcpy(d->t_offsets.get(), toff.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice));
-      FEM_CUDA_CHECK(cudaMemcpy(d->t_indices.get(), tidx.data(), n_t * sizeof(int), cudaMemcpyHostToDevice));
-    }
-    *out = new fem_b200_restriction_s{std::move(d)};
+    *out = new fem_b200_restriction_s{
+        make_offset_restriction(num_elem, elem_size, num_comp, comp_stride, l_size, offsets, offsets, scatter_mode, 0)};
   });
 }
 
@@ -802,7 +786,7 @@ int fem_b200_mass_build(fem_b200_restriction rx, fem_b200_basis bx, const double
       throw unsupported_error("mass build: no device kernel for " + shape_str(b.dim, b.P, b.Q) +
                               " (P in 2..8, Q in P..P+2; dim 3 with P = 8 up to Q = 9)");
     DeviceGuard g(r.device);
-    dispatch().build[b.dim - 1][b.P][b.Q - b.P](b, r, x, qdata, as_stream(stream));
+    mass_build_impl(b, r, x, qdata, as_stream(stream));
   });
 }
 
@@ -822,38 +806,8 @@ int fem_b200_mass_create(fem_b200_restriction ru, fem_b200_basis bu, const doubl
     if (!fused_supported(b.dim, b.P, b.Q))
       throw unsupported_error("operator_apply: no fused device kernel for " + shape_str(b.dim, b.P, b.Q) +
                               " (P in 2..8, Q in P..P+2)");
-    auto p = std::make_unique<MassPlan>();
-    p->device = r->device;
-    DeviceGuard g(p->device);
-    p->dim = b.dim, p->P = b.P, p->Q = b.Q, p->num_comp = b.num_comp;
-    p->qf = qf;
-    p->comp_run = qf == FEM_B200_QF_APPLY_MASS ? 1 : b.num_comp;
-    p->scatter_mode = r->scatter_mode;
-    p->num_elem = r->num_elem, p->l_size = r->l_size, p->es = r->elem_size, p->nq = int(nq);
-    p->comp_stride = r->comp_stride;
-    p->basis = b;
-    p->r = r;
-    p->tile_e = b.dim == 3 ? 8 : (b.dim == 2 ? 32 : 128);
-    p->n_tiles = (int64_t(p->num_elem) + p->tile_e - 1) / p->tile_e;
-    // an even number of tiles, so a kernel taking two tiles per CTA stays inside
-    const int64_t ne_pad = ((p->n_tiles + 1) / 2) * 2 * p->tile_e;
-    p->offs_t.alloc(size_t(ne_pad * p->es));
-    p->qd_t.alloc(size_t(ne_pad * p->nq));
-    tile_offsets_kernel<<<grid_for(ne_pad * p->es, 256), 256>>>(r->offsets.get(), p->num_elem, p->es, p->tile_e,
-                                                                ne_pad * p->es, p->offs_t.get());
-    FEM_LAUNCH_CHECK();
-    tile_qdata_kernel<<<grid_for(ne_pad * p->nq, 256), 256>>>(qdata, p->num_elem, p->Q, p->nq, p->tile_e,
-                                                              ne_pad * p->nq, p->qd_t.get());
-    FEM_LAUNCH_CHECK();
-    if (p->scatter_mode == FEM_B200_SCATTER_DETERMINISTIC) p->evec.alloc(size_t(int64_t(p->comp_run) * p->es * p->num_elem));
-    p->status.alloc(1);
-    FEM_CUDA_CHECK(cudaMemset(p->status.get(), 0, sizeof(int)));
-    p->launch_simple = dispatch().apply[b.dim - 1][b.P][b.Q - b.P];
-    p->launch_pipe = b.dim == 3 ? dispatch().apply3_pipe[b.P][b.Q - b.P] : nullptr;
-    p->launch_x2 = b.dim == 3 ? dispatch().apply3_x2[b.P][b.Q - b.P] : nullptr;
-    p->launch_pf = b.dim == 3 ? dispatch().apply3_pf[b.P][b.Q - b.P] : nullptr;
-    p->launch_occ = b.dim == 3 ? dispatch().apply3_occ[b.P][b.Q - b.P] : nullptr;
-    p->launch = auto_kernel(*p);
+    DeviceGuard g(r->device);
+    auto p = make_mass_plan(r, b, qdata, qf, 0);
     FEM_CUDA_CHECK(cudaDeviceSynchronize());
     *out = new fem_b200_mass_s{std::move(p)};
   });
@@ -867,14 +821,92 @@ int fem_b200_mass_destroy(fem_b200_mass op) {
 
 namespace fem_b200 {
 // Reads and clears the plan's device status word (the caller has synchronised).
-void check_status(MassPlan& p) {
+void check_status(MassPlan& p, cudaStream_t s) {
   int st = 0;
-  FEM_CUDA_CHECK(cudaMemcpy(&st, p.status.get(), sizeof(int), cudaMemcpyDeviceToHost));
+  if (s) {  // pageable destination: returns once the copy is done
+    FEM_CUDA_CHECK(cudaMemcpyAsync(&st, p.status.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+  } else {
+    FEM_CUDA_CHECK(cudaMemcpy(&st, p.status.get(), sizeof(int), cudaMemcpyDeviceToHost));
+  }
   if (st) {
-    FEM_CUDA_CHECK(cudaMemset(p.status.get(), 0, sizeof(int)));
+    FEM_CUDA_CHECK(cudaMemsetAsync(p.status.get(), 0, sizeof(int), s));
     throw cuda_error("operator_apply: a bounded wait in the mass kernel ran out (status " + std::to_string(st) +
                      "); the result is not valid");
   }
+}
+
+// ---- stream-ordered cores of the create / build entry points ---------------
+std::shared_ptr<RestrictionData> make_offset_restriction(int num_elem, int elem_size, int num_comp, int comp_stride,
+                                                         int l_size, const int* offs, const int* host_offsets,
+                                                         int scatter_mode, cudaStream_t s) {
+  const int64_t n_t = int64_t(num_elem) * elem_size;
+  auto d = std::make_shared<RestrictionData>();
+  d->device = current_device();
+  d->num_elem = num_elem, d->elem_size = elem_size, d->num_comp = num_comp;
+  d->comp_stride = comp_stride;
+  d->l_size = l_size;
+  d->e_size = int64_t(num_comp) * n_t;
+  d->scatter_mode = scatter_mode;
+  d->offsets.alloc(size_t(n_t));
+  FEM_CUDA_CHECK(cudaMemcpyAsync(d->offsets.get(), offs, n_t * sizeof(int), cudaMemcpyDefault, s));
+  std::vector<int> lvi, toff, tidx;
+  if (scatter_mode == FEM_B200_SCATTER_DETERMINISTIC) {
+    require(host_offsets != nullptr, "elem_restriction_create: the deterministic scatter needs host offsets");
+    lvi.resize(size_t(l_size)), toff.resize(size_t(l_size) + 1), tidx.resize(size_t(n_t));
+    const int n = transpose_map(num_elem, elem_size, l_size, host_offsets, lvi.data(), toff.data(), tidx.data());
+    d->num_nodes = n;
+    d->l_vec_indices.alloc(size_t(n));
+    d->t_offsets.alloc(size_t(n) + 1);
+    d->t_indices.alloc(size_t(n_t));
+    FEM_CUDA_CHECK(cudaMemcpyAsync(d->l_vec_indices.get(), lvi.data(), n * sizeof(int), cudaMemcpyHostToDevice, s));
+    FEM_CUDA_CHECK(cudaMemcpyAsync(d->t_offsets.get(), toff.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice, s));
+    FEM_CUDA_CHECK(cudaMemcpyAsync(d->t_indices.get(), tidx.data(), n_t * sizeof(int), cudaMemcpyHostToDevice, s));
+  }
+  FEM_CUDA_CHECK(cudaStreamSynchronize(s));  // the host vectors go out of scope
+  return d;
+}
+
+void mass_build_impl(const BasisData& b, const RestrictionData& r, const double* x, double* qdata, cudaStream_t s) {
+  dispatch().build[b.dim - 1][b.P][b.Q - b.P](b, r, x, qdata, s);
+}
+
+std::unique_ptr<MassPlan> make_mass_plan(const std::shared_ptr<RestrictionData>& r, const BasisData& b,
+                                         const double* qdata, int qf, cudaStream_t s) {
+  const int64_t nq = ipow(b.Q, b.dim);
+  auto p = std::make_unique<MassPlan>();
+  p->device = r->device;
+  p->dim = b.dim, p->P = b.P, p->Q = b.Q, p->num_comp = b.num_comp;
+  p->qf = qf;
+  p->comp_run = qf == FEM_B200_QF_APPLY_MASS ? 1 : b.num_comp;
+  p->scatter_mode = r->scatter_mode;
+  p->num_elem = r->num_elem, p->l_size = r->l_size, p->es = r->elem_size, p->nq = int(nq);
+  p->comp_stride = r->comp_stride;
+  p->basis = b;
+  p->r = r;
+  p->tile_e = b.dim == 3 ? 8 : (b.dim == 2 ? 32 : 128);
+  p->n_tiles = (int64_t(p->num_elem) + p->tile_e - 1) / p->tile_e;
+  // an even number of tiles, so a kernel taking two tiles per CTA stays inside
+  const int64_t ne_pad = ((p->n_tiles + 1) / 2) * 2 * p->tile_e;
+  p->offs_t.alloc(size_t(ne_pad * p->es));
+  p->qd_t.alloc(size_t(ne_pad * p->nq));
+  tile_offsets_kernel<<<grid_for(ne_pad * p->es, 256), 256, 0, s>>>(r->offsets.get(), p->num_elem, p->es,
+                                                                     p->tile_e, ne_pad * p->es, p->offs_t.get());
+  FEM_LAUNCH_CHECK();
+  tile_qdata_kernel<<<grid_for(ne_pad * p->nq, 256), 256, 0, s>>>(qdata, p->num_elem, p->Q, p->nq, p->tile_e,
+                                                                   ne_pad * p->nq, p->qd_t.get());
+  FEM_LAUNCH_CHECK();
+  if (p->scatter_mode == FEM_B200_SCATTER_DETERMINISTIC)
+    p->evec.alloc(size_t(int64_t(p->comp_run) * p->es * p->num_elem));
+  p->status.alloc(1);
+  FEM_CUDA_CHECK(cudaMemsetAsync(p->status.get(), 0, sizeof(int), s));
+  p->launch_simple = dispatch().apply[b.dim - 1][b.P][b.Q - b.P];
+  p->launch_pipe = b.dim == 3 ? dispatch().apply3_pipe[b.P][b.Q - b.P] : nullptr;
+  p->launch_x2 = b.dim == 3 ? dispatch().apply3_x2[b.P][b.Q - b.P] : nullptr;
+  p->launch_pf = b.dim == 3 ? dispatch().apply3_pf[b.P][b.Q - b.P] : nullptr;
+  p->launch_occ = b.dim == 3 ? dispatch().apply3_occ[b.P][b.Q - b.P] : nullptr;
+  p->launch = auto_kernel(*p);
+  FEM_CUDA_CHECK(cudaStreamSynchronize(s));
+  return p;
 }
 
 void mass_apply_impl(MassPlan& p, const double* u, double* v, bool zero, cudaStream_t s) {

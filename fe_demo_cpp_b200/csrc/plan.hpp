@@ -22,6 +22,30 @@
 namespace fem_b200 {
 
 // ---------------------------------------------------------------------------
+// Stream-ordered allocation.  Inside an AllocScope, the DevBufs a thread
+// allocates come from `pool` in `stream` order (cudaMallocFromPoolAsync) and
+// are returned in that stream's order when released (cudaFreeAsync), so a
+// request that builds and frees its buffers does not synchronise the device
+// under the other requests' kernels (cudaFree would).
+// ---------------------------------------------------------------------------
+struct AllocCtx {
+  cudaStream_t stream = nullptr;
+  cudaMemPool_t pool = nullptr;
+};
+inline AllocCtx*& alloc_ctx() {
+  static thread_local AllocCtx* ctx = nullptr;
+  return ctx;
+}
+struct AllocScope {
+  AllocCtx ctx;
+  AllocCtx* prev;
+  AllocScope(cudaStream_t s, cudaMemPool_t pool) : ctx{s, pool}, prev(alloc_ctx()) { alloc_ctx() = &ctx; }
+  ~AllocScope() { alloc_ctx() = prev; }
+  AllocScope(const AllocScope&) = delete;
+  AllocScope& operator=(const AllocScope&) = delete;
+};
+
+// ---------------------------------------------------------------------------
 // RAII device buffer (move-only), the reference's DeviceArray semantics
 // (include/cuda/device-array.hpp:18-95) without the synchronous copies.
 // ---------------------------------------------------------------------------
@@ -33,11 +57,11 @@ class DevBuf {
   ~DevBuf() { release(); }
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
-  DevBuf(DevBuf&& o) noexcept : p_(o.p_), n_(o.n_) { o.p_ = nullptr, o.n_ = 0; }
+  DevBuf(DevBuf&& o) noexcept : p_(o.p_), n_(o.n_), s_(o.s_), async_(o.async_) { o.p_ = nullptr, o.n_ = 0; }
   DevBuf& operator=(DevBuf&& o) noexcept {
     if (this != &o) {
       release();
-      p_ = o.p_, n_ = o.n_;
+      p_ = o.p_, n_ = o.n_, s_ = o.s_, async_ = o.async_;
       o.p_ = nullptr, o.n_ = 0;
     }
     return *this;
@@ -45,7 +69,13 @@ class DevBuf {
   void alloc(size_t n) {
     release();
     if (n == 0) return;
-    FEM_CUDA_CHECK(cudaMalloc(&p_, n * sizeof(T)));
+    if (AllocCtx* c = alloc_ctx()) {
+      FEM_CUDA_CHECK(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&p_), n * sizeof(T), c->pool, c->stream));
+      s_ = c->stream, async_ = true;
+    } else {
+      FEM_CUDA_CHECK(cudaMalloc(&p_, n * sizeof(T)));
+      s_ = nullptr, async_ = false;
+    }
     n_ = n;
   }
   T* get() const { return p_; }
@@ -54,11 +84,18 @@ class DevBuf {
 
  private:
   void release() noexcept {
-    if (p_) (void)cudaFree(p_);
+    if (p_) {
+      if (async_)
+        (void)cudaFreeAsync(p_, s_);
+      else
+        (void)cudaFree(p_);
+    }
     p_ = nullptr, n_ = 0;
   }
   T* p_ = nullptr;
   size_t n_ = 0;
+  cudaStream_t s_ = nullptr;
+  bool async_ = false;
 };
 
 // RAII page-locked host buffer.
@@ -169,6 +206,7 @@ struct MassPlan {
   DevBuf<double> part;                    // per-CTA partial sums of the grid reductions
   DevBuf<CgScalars> cg_st;                // device-resident solver scalars
   PinnedBuf<CgScalars> cg_host;           // their host copy
+  CgScalars* cg_host_ext = nullptr;       // or a page-locked copy owned by the caller (a server slot)
   DevBuf<float> qd_t32, dinv32, evec32;   // FP32 copies for the inner solves
   DevBuf<float> f_r, f_p, f_s, f_w, f_x;  // FP32 Krylov vectors
 };
@@ -224,9 +262,30 @@ void set_smem(K kernel, int bytes, std::atomic<uint64_t>& done) {
 }
 
 // Defined in device.cu.
-void check_status(MassPlan& p);
+void check_status(MassPlan& p, cudaStream_t s = nullptr);
 void mass_apply_impl(MassPlan& p, const double* u, double* v, bool zero, cudaStream_t s);
 std::string shape_str(int dim, int P, int Q);
+// A fused apply and build kernel exist for (dim, P, Q).
+bool device_path_supported(int dim, int P, int Q);
+// An offset restriction over device offsets `offs` (its copy is taken);
+// host_offsets (the same values) are needed for the deterministic scatter's
+// transpose map, else may be null.  Work in `s`, synchronised before return.
+std::shared_ptr<RestrictionData> make_offset_restriction(int num_elem, int elem_size, int num_comp, int comp_stride,
+                                                         int l_size, const int* offs, const int* host_offsets,
+                                                         int scatter_mode, cudaStream_t s);
+// qdata = det(J) w from coordinates x (the fused build kernel), in `s`.
+void mass_build_impl(const BasisData& b, const RestrictionData& r, const double* x, double* qdata, cudaStream_t s);
+// A mass plan (tiled offsets and qdata) in `s`, synchronised before return.
+std::unique_ptr<MassPlan> make_mass_plan(const std::shared_ptr<RestrictionData>& r, const BasisData& b,
+                                         const double* qdata, int qf, cudaStream_t s);
+
+// Defined in solver.cu.
+struct SolveStats {
+  int iterations = 0, refinements = 0;
+  double rel_residual = 0.0;
+};
+SolveStats mass_solve_impl(MassPlan& p, const double* f, double* u, double rtol, int max_iter, int precision,
+                           cudaStream_t s);
 
 }  // namespace fem_b200
 

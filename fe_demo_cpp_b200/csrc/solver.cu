@@ -489,7 +489,7 @@ void ensure_solver_state(MassPlan& p, bool fp32, cudaStream_t s) {
     p.part.alloc(2 * size_t(std::max<int64_t>(p.n_tiles, 148 * 8)));
     p.cg_st.alloc(1);
     FEM_CUDA_CHECK(cudaMemsetAsync(p.cg_st.get(), 0, sizeof(CgScalars), s));
-    p.cg_host.alloc(1);
+    if (!p.cg_host_ext) p.cg_host.alloc(1);
   }
   if (fp32 && p.qd_t32.size() != p.qd_t.size()) {
     p.qd_t32.alloc(p.qd_t.size());
@@ -505,10 +505,12 @@ void ensure_solver_state(MassPlan& p, bool fp32, cudaStream_t s) {
 }
 
 // The host's copy of the device scalars (synchronises the stream).
+CgScalars* host_scalars(MassPlan& p) { return p.cg_host_ext ? p.cg_host_ext : p.cg_host.get(); }
+
 const CgScalars& read_scalars(MassPlan& p, cudaStream_t s) {
-  FEM_CUDA_CHECK(cudaMemcpyAsync(p.cg_host.get(), p.cg_st.get(), sizeof(CgScalars), cudaMemcpyDeviceToHost, s));
+  FEM_CUDA_CHECK(cudaMemcpyAsync(host_scalars(p), p.cg_st.get(), sizeof(CgScalars), cudaMemcpyDeviceToHost, s));
   FEM_CUDA_CHECK(cudaStreamSynchronize(s));
-  return *p.cg_host.get();
+  return *host_scalars(p);
 }
 
 inline bool aligned16(const void* ptr) { return (reinterpret_cast<uintptr_t>(ptr) & 15) == 0; }
@@ -566,7 +568,7 @@ CgScalars krylov_solve(MassPlan& p, const Krylov<T>& k, const double* b, double 
     if (st.done) break;
     if (queued > max_it + 64) throw cuda_error("mass solve: the device iteration count did not advance");
   }
-  const CgScalars st = *p.cg_host.get();
+  const CgScalars st = *host_scalars(p);
   if (st.done == 3 && st.iters == 0)
     throw cuda_error("mass solve: breakdown, (u, M u) <= 0: the operator is not positive definite on this "
                      "right-hand side");
@@ -586,6 +588,48 @@ double outer_residual(MassPlan& p, const double* f, const double* u, cudaStream_
 // The FP32 inner solve's relative tolerance: what the last cycle still needs
 // (with a factor 2 margin), but not below what FP32 Krylov vectors attain.
 constexpr double kInnerFloor = 5e-6;
+
+SolveStats mass_solve_impl(MassPlan& p, const double* f, double* u, double rtol, int max_iter, int precision,
+                           cudaStream_t s) {
+  const bool fp32 = precision == FEM_B200_SOLVE_FP32_IR;
+  ensure_solver_state(p, fp32, s);
+  const SolveDispatch& d = solve_dispatch();
+  const int di = p.Q - p.P;
+  int total_it = 0, outer = 0;
+  double nf = 0.0, nr = 0.0;
+  if (!fp32) {
+    const Krylov<double> k{u, p.cg_r.get(), p.cg_p.get(), p.cg_s.get(), p.cg_w.get(), p.evec.get(),
+                           p.dinv.get(), p.qd_t.get(), d.cg64[p.P][di]};
+    const CgScalars st = krylov_solve<double>(p, k, f, 1.0, rtol, max_iter, s);
+    total_it = st.iters;
+    nf = std::sqrt(st.rr0);
+    nr = outer_residual(p, f, u, s);  // the true FP64 residual
+  } else {
+    // FP64 outer loop: r = f - M u in FP64, correction from FP32 PCG on r / ||r||.
+    nf = outer_residual(p, f, nullptr, s);
+    FEM_CUDA_CHECK(cudaMemsetAsync(u, 0, size_t(p.l_size) * sizeof(double), s));
+    nr = nf;
+    const Krylov<float> k{p.f_x.get(), p.f_r.get(), p.f_p.get(), p.f_s.get(), p.f_w.get(), p.evec32.get(),
+                          p.dinv32.get(), p.qd_t32.get(), d.cg32[p.P][di]};
+    while (nr > rtol * nf && total_it < max_iter && outer < 50) {
+      const double inner = std::min(0.5, std::max(kInnerFloor, 0.5 * rtol * nf / nr));
+      const CgScalars st = krylov_solve<float>(p, k, p.cg_r.get(), 1.0 / nr, inner, max_iter - total_it, s);
+      total_it += st.iters;
+      ++outer;
+      add_scaled_kernel<<<red_grid(p.l_size), 256, 0, s>>>(p.l_size, nr, p.f_x.get(), u);
+      FEM_LAUNCH_CHECK();
+      const double prev = nr;
+      nr = outer_residual(p, f, u, s);
+      if (!(nr < prev)) break;  // no progress: the FP32 solve has stalled
+    }
+  }
+  check_status(p, s);
+  SolveStats out;
+  out.iterations = total_it;
+  out.refinements = outer;
+  out.rel_residual = nf > 0.0 ? nr / nf : 0.0;
+  return out;
+}
 
 }  // namespace fem_b200
 
@@ -619,43 +663,10 @@ int fem_b200_mass_solve(fem_b200_mass op, const double* f, int64_t n_f, double* 
           "mass solve: the reference apply_mass leaves components 1.. out (a singular operator); use "
           "FEM_B200_QF_APPLY_MASS_VECTOR for a multi-component solve");
     DeviceGuard g(p.device);
-    cudaStream_t s = as_stream(stream);
-    const bool fp32 = precision == FEM_B200_SOLVE_FP32_IR;
-    ensure_solver_state(p, fp32, s);
-    const SolveDispatch& d = solve_dispatch();
-    const int di = p.Q - p.P;
-    int total_it = 0, outer = 0;
-    double nf = 0.0, nr = 0.0;
-    if (!fp32) {
-      const Krylov<double> k{u, p.cg_r.get(), p.cg_p.get(), p.cg_s.get(), p.cg_w.get(), p.evec.get(),
-                             p.dinv.get(), p.qd_t.get(), d.cg64[p.P][di]};
-      const CgScalars st = krylov_solve<double>(p, k, f, 1.0, rtol, max_iter, s);
-      total_it = st.iters;
-      nf = std::sqrt(st.rr0);
-      nr = outer_residual(p, f, u, s);  // the true FP64 residual
-    } else {
-      // FP64 outer loop: r = f - M u in FP64, correction from FP32 PCG on r / ||r||.
-      nf = outer_residual(p, f, nullptr, s);
-      FEM_CUDA_CHECK(cudaMemsetAsync(u, 0, size_t(p.l_size) * sizeof(double), s));
-      nr = nf;
-      const Krylov<float> k{p.f_x.get(), p.f_r.get(), p.f_p.get(), p.f_s.get(), p.f_w.get(), p.evec32.get(),
-                            p.dinv32.get(), p.qd_t32.get(), d.cg32[p.P][di]};
-      while (nr > rtol * nf && total_it < max_iter && outer < 50) {
-        const double inner = std::min(0.5, std::max(kInnerFloor, 0.5 * rtol * nf / nr));
-        const CgScalars st = krylov_solve<float>(p, k, p.cg_r.get(), 1.0 / nr, inner, max_iter - total_it, s);
-        total_it += st.iters;
-        ++outer;
-        add_scaled_kernel<<<red_grid(p.l_size), 256, 0, s>>>(p.l_size, nr, p.f_x.get(), u);
-        FEM_LAUNCH_CHECK();
-        const double prev = nr;
-        nr = outer_residual(p, f, u, s);
-        if (!(nr < prev)) break;  // no progress: the FP32 solve has stalled
-      }
-    }
-    check_status(p);
-    if (iterations) *iterations = total_it;
-    if (refinements) *refinements = outer;
-    if (rel_residual) *rel_residual = nf > 0.0 ? nr / nf : 0.0;
+    const SolveStats st = mass_solve_impl(p, f, u, rtol, max_iter, precision, as_stream(stream));
+    if (iterations) *iterations = st.iterations;
+    if (refinements) *refinements = st.refinements;
+    if (rel_residual) *rel_residual = st.rel_residual;
   });
 }
 

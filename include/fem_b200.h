@@ -37,6 +37,7 @@ extern "C" {
 #define FEM_B200_ERROR_ARGUMENT 1    /* bad size / index / mode (std::invalid_argument) */
 #define FEM_B200_ERROR_CUDA 2        /* a CUDA call or a device status failed */
 #define FEM_B200_ERROR_UNSUPPORTED 3 /* valid, but not on the device path (no CPU fallback) */
+#define FEM_B200_NOT_READY 4         /* fem_b200_server_wait: not finished within the timeout */
 
 /* ---- enums, numbered as the reference's ---------------------------------- */
 /* ContractMode, include/transpose-mode.hpp:13 */
@@ -68,6 +69,7 @@ typedef struct fem_b200_restriction_s *fem_b200_restriction;
 typedef struct fem_b200_basis_s *fem_b200_basis;
 typedef struct fem_b200_mass_s *fem_b200_mass;
 typedef struct fem_b200_batch_s *fem_b200_batch;
+typedef struct fem_b200_server_s *fem_b200_server;
 
 /* Message of this thread's last failure ("" if none). */
 const char *fem_b200_last_error(void);
@@ -360,6 +362,62 @@ int fem_b200_batch_autotune(fem_b200_batch b, int reps, void *stream);
 int fem_b200_batch_info(fem_b200_batch b, int *num_classes, int64_t *total_tiles, int64_t *total_dofs,
                         int *graph_kernels, int *persistent_classes);
 int fem_b200_batch_destroy(fem_b200_batch b);
+
+/* ---- served solves (no reference counterpart) ------------------------------
+ * A request loop over a device-memory budget: each request is one mass solve
+ * M u = f (vector mass, num_comp 1..3) on its own mesh.  Requests are admitted
+ * in arrival order as soon as one of `slots` workers is free and the
+ * request's device-memory estimate (mesh, qdata, Krylov vectors, set-up
+ * temporaries) fits in what the budget has left; admitted requests keep
+ * their data resident until they finish and run concurrently, each worker on
+ * its own CUDA stream with stream-ordered allocation, so their kernels
+ * overlap.  A result does not depend on the mix it ran in (bitwise so with
+ * the deterministic scatter). */
+#define FEM_B200_REQUEST_BOX 0  /* box [0,1]^dim generated on the device */
+#define FEM_B200_REQUEST_MESH 1 /* offsets / coordinates / f from the host */
+typedef struct {
+  int kind;
+  int dim, P, Q, num_comp;
+  /* BOX: elements per direction, interior vertices moved by U[-perturb h,
+   * perturb h] per coordinate, f ~ U[-1, 1]; mesh and f from `seed` */
+  int shape[3];
+  double perturb;
+  uint64_t seed;
+  /* MESH (host arrays, valid until the request completes): offsets
+   * [num_elem][P^dim], coordinates blocked [dim][num_nodes], f blocked
+   * [num_comp][num_nodes] */
+  int num_elem, num_nodes;
+  const int *offsets;
+  const double *coords;
+  const double *f;
+  /* the solve: as fem_b200_mass_solve */
+  double rtol;
+  int max_iter, precision, scatter_mode;
+  /* optional host outputs (num_comp * num_nodes doubles, valid until the
+   * request completes): the solution, and the right-hand side used */
+  double *u_out;
+  double *f_out;
+} fem_b200_request;
+typedef struct {
+  int status; /* FEM_B200_SUCCESS or the error of this request (message) */
+  int iterations, refinements;
+  double rel_residual; /* ||f - M u|| / ||f||, FP64 */
+  double t_submit, t_start, t_end; /* seconds on the server's clock */
+  int64_t dofs;         /* num_comp * num_nodes */
+  int64_t device_bytes; /* reserved from the budget while it ran */
+  char message[256];
+} fem_b200_result;
+int fem_b200_server_create(int slots, int64_t hbm_budget_bytes, fem_b200_server *out);
+/* Queue a request; ARGUMENT error if it alone exceeds the budget. */
+int fem_b200_server_submit(fem_b200_server s, const fem_b200_request *req, int64_t *id);
+/* Wait up to timeout_s seconds (< 0: no limit) for request `id`; on success
+ * the result is written and the id forgotten; FEM_B200_NOT_READY on timeout. */
+int fem_b200_server_wait(fem_b200_server s, int64_t id, double timeout_s, fem_b200_result *result);
+/* Any output may be NULL. */
+int fem_b200_server_stats(fem_b200_server s, int64_t *submitted, int64_t *completed, int *running, int64_t *pending,
+                          int64_t *bytes_in_use, int64_t *bytes_peak);
+/* Finishes every queued request, then stops the workers. */
+int fem_b200_server_destroy(fem_b200_server s);
 
 /* Synchronise `stream` and report a device-side failure of the plan's kernels
  * (a bounded wait that ran out) as FEM_B200_ERROR_CUDA.  fem_b200_mass_apply_host

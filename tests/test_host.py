@@ -137,3 +137,27 @@ def test_mesh_generator_is_a_valid_box(fem):
     o = m.offsets.reshape(m.num_elem, 4, 4, 4)
     assert np.array_equal(o[0, :, :, 3], o[1, :, :, 0])
     assert box_mesh((4, 3, 2), 4, seed=2).digest() == m.digest()
+
+
+def test_server_struct_layouts_match_the_header(tmp_path):
+    """The ctypes mirrors of fem_b200_request / fem_b200_result have the C
+    header's field offsets and sizes (compiled with gcc, no GPU)."""
+    import ctypes as C
+    import subprocess
+    from fe_demo_cpp_b200.api import _Request, _Result
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "fem_b200.h"', 'int main(void) {']
+    for ty, cls in (("fem_b200_request", _Request), ("fem_b200_result", _Result)):
+        lines.append(f'printf("{ty} %zu\\n", sizeof({ty}));')
+        for name, _ in cls._fields_:
+            lines.append(f'printf("{ty}.{name} %zu\\n", offsetof({ty}, {name}));')
+    lines += ["return 0;", "}"]
+    src, exe = tmp_path / "layout.c", tmp_path / "layout"
+    src.write_text("\n".join(lines))
+    subprocess.run(["gcc", "-I", os.path.join(root, "include"), str(src), "-o", str(exe)], check=True)
+    out = dict(line.split() for line in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                       check=True).stdout.splitlines())
+    for ty, cls in (("fem_b200_request", _Request), ("fem_b200_result", _Result)):
+        assert int(out[ty]) == C.sizeof(cls)
+        for name, _ in cls._fields_:
+            assert int(out[f"{ty}.{name}"]) == getattr(cls, name).offset, (ty, name)
