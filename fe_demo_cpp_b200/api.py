@@ -354,12 +354,12 @@ class Batch(_Handle):
         call("fem_b200_batch_autotune", self.h, int(reps), _stream(stream))
 
     def info(self) -> dict:
-        nc, gk, pc = C.c_int(0), C.c_int(0), C.c_int(0)
+        nc, gk, pc, br = C.c_int(0), C.c_int(0), C.c_int(0), C.c_int(0)
         tiles, dofs = C.c_int64(0), C.c_int64(0)
         call("fem_b200_batch_info", self.h, C.addressof(nc), C.addressof(tiles), C.addressof(dofs),
-             C.addressof(gk), C.addressof(pc))
+             C.addressof(gk), C.addressof(pc), C.addressof(br))
         return {"classes": nc.value, "tiles": tiles.value, "dofs": dofs.value, "graph_kernels": gk.value,
-                "persistent_classes": pc.value}
+                "persistent_classes": pc.value, "graph_branches": br.value}
 
 
 class _Request(C.Structure):

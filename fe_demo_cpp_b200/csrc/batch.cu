@@ -140,7 +140,7 @@ constexpr int batch_min_blocks(int P, int threads, int ncb) {
   const int regs = P == 6 ? 80 : ncb == 3 ? 72 : 56;
   for (int b = cap; b > 1; --b)
     if (b * threads <= 2048 && 65536 / (b * threads) >= regs) return b;
-  return 1;
+  return P >= 8 ? 1 : 0;  // as the single-mesh kernel (plain_min_blocks)
 }
 
 template <int P, int Q, class T, int NCB>
@@ -235,6 +235,7 @@ struct BatchPlan {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   int graph_kernels = 0;
+  int branches = 1;  // parallel graph branches (classes run concurrently), autotuned
 
   ~BatchPlan() {
     int prev = -1;
@@ -258,8 +259,8 @@ struct BatchPlan {
 };
 
 // Every v_i zeroed, then every class (the heaviest first, round-robin over
-// the streams, which fork from and join into s0).
-void enqueue_batch(BatchPlan& b, cudaStream_t s0, bool fork) {
+// `branches` streams, which fork from and join into s0).
+void enqueue_batch(BatchPlan& b, cudaStream_t s0, int branches) {
   const unsigned ops = unsigned(b.ops.size());
   const unsigned zx = unsigned(std::max<int64_t>(1, std::min<int64_t>(64, (b.max_l_size + 2047) / 2048)));
   if (b.precision == FEM_B200_PRECISION_FP32)
@@ -268,7 +269,8 @@ void enqueue_batch(BatchPlan& b, cudaStream_t s0, bool fork) {
     batch_zero_kernel<double><<<dim3(zx, ops), 256, 0, s0>>>(
         reinterpret_cast<const BatchMesh<double>*>(b.meshes.get()));
   FEM_LAUNCH_CHECK();
-  const int ns = fork ? int(std::min<size_t>(kBatchMaxStreams, b.classes.size())) : 1;
+  const int ns = int(std::min<size_t>(size_t(std::max(branches, 1)),
+                                       std::min<size_t>(kBatchMaxStreams, b.classes.size())));
   if (ns > 1) {
     FEM_CUDA_CHECK(cudaEventRecord(b.fork, s0));
     for (int i = 1; i < ns; ++i) FEM_CUDA_CHECK(cudaStreamWaitEvent(b.streams[i], b.fork, 0));
@@ -291,7 +293,7 @@ void capture_batch(BatchPlan& b) {
   cudaStream_t s0 = b.streams[0];
   FEM_CUDA_CHECK(cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal));
   try {
-    enqueue_batch(b, s0, true);
+    enqueue_batch(b, s0, b.branches);
   } catch (...) {
     cudaGraph_t g = nullptr;
     (void)cudaStreamEndCapture(s0, &g);
@@ -302,6 +304,29 @@ void capture_batch(BatchPlan& b) {
   FEM_CUDA_CHECK(cudaGraphInstantiate(&b.exec, b.graph, 0));
   b.graph_kernels = 1 + int(b.classes.size());
 }
+
+// Two timing events (RAII); time(s, f) = device ms of what f enqueues in s.
+struct EventPair {
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  EventPair() {
+    FEM_CUDA_CHECK(cudaEventCreate(&e0));
+    FEM_CUDA_CHECK(cudaEventCreate(&e1));
+  }
+  ~EventPair() {
+    (void)cudaEventDestroy(e0);
+    (void)cudaEventDestroy(e1);
+  }
+  template <class F>
+  float time(cudaStream_t s, F&& f) {
+    FEM_CUDA_CHECK(cudaEventRecord(e0, s));
+    f();
+    FEM_CUDA_CHECK(cudaEventRecord(e1, s));
+    FEM_CUDA_CHECK(cudaEventSynchronize(e1));
+    float ms = 0.0f;
+    FEM_CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+    return ms;
+  }
+};
 
 template <class T>
 void write_descriptors(BatchPlan& b, const void* const* u, void* const* v) {
@@ -424,12 +449,12 @@ int fem_b200_batch_apply(fem_b200_batch batch, int use_graph, void* stream) {
     DeviceGuard g(b.device);
     cudaStream_t s = as_stream(stream);
     if (!use_graph) {
-      enqueue_batch(b, s, false);
+      enqueue_batch(b, s, 1);
       return;
     }
     if (!b.exec) {
       // the kernels' attributes are set by one direct pass before the capture
-      enqueue_batch(b, s, false);
+      enqueue_batch(b, s, 1);
       FEM_CUDA_CHECK(cudaStreamSynchronize(s));
       capture_batch(b);
     }
@@ -445,40 +470,42 @@ int fem_b200_batch_autotune(fem_b200_batch batch, int reps, void* stream) {
     require(reps >= 1, "batch autotune: reps must be positive");
     DeviceGuard g(b.device);
     cudaStream_t s = as_stream(stream);
-    enqueue_batch(b, s, false);  // v zeroed; attributes set
-    cudaEvent_t e0, e1;
-    FEM_CUDA_CHECK(cudaEventCreate(&e0));
-    FEM_CUDA_CHECK(cudaEventCreate(&e1));
-    try {
-      for (BatchClass& c : b.classes) {
-        float best = 0.0f;
-        for (int sched = 0; sched < 2; ++sched) {
-          c.launch(c, b.meshes.get(), sched == 0 ? unsigned(c.n_tiles) : 0u, s);  // warm-up
-          FEM_CUDA_CHECK(cudaEventRecord(e0, s));
-          for (int r = 0; r < reps; ++r) c.launch(c, b.meshes.get(), sched == 0 ? unsigned(c.n_tiles) : 0u, s);
-          FEM_CUDA_CHECK(cudaEventRecord(e1, s));
-          FEM_CUDA_CHECK(cudaEventSynchronize(e1));
-          float ms = 0.0f;
-          FEM_CUDA_CHECK(cudaEventElapsedTime(&ms, e0, e1));
-          if (sched == 0 || ms < best) best = ms, c.schedule = sched;
-        }
+    enqueue_batch(b, s, 1);  // v zeroed; attributes set
+    EventPair ev;
+    // each class: one CTA per tile, or the persistent grid
+    for (BatchClass& c : b.classes) {
+      float best = 0.0f;
+      for (int sched = 0; sched < 2; ++sched) {
+        const unsigned grid = sched == 0 ? unsigned(c.n_tiles) : 0u;
+        c.launch(c, b.meshes.get(), grid, s);  // warm-up
+        const float ms = ev.time(s, [&] {
+          for (int r = 0; r < reps; ++r) c.launch(c, b.meshes.get(), grid, s);
+        });
+        if (sched == 0 || ms < best) best = ms, c.schedule = sched;
       }
-    } catch (...) {
-      (void)cudaEventDestroy(e0);
-      (void)cudaEventDestroy(e1);
-      throw;
     }
-    (void)cudaEventDestroy(e0);
-    (void)cudaEventDestroy(e1);
-    // the timing runs accumulated into v; leave the v_i = M_i u_i
-    enqueue_batch(b, s, false);
+    // then the graph's parallel branches: classes that run concurrently
+    // contend for HBM, which pays off in some precisions only
+    float best = 0.0f;
+    int best_branches = 1;
+    for (int nb : {1, 2, 4}) {
+      b.branches = nb;
+      capture_batch(b);
+      FEM_CUDA_CHECK(cudaGraphLaunch(b.exec, s));  // warm-up
+      const float ms = ev.time(s, [&] {
+        for (int r = 0; r < reps; ++r) FEM_CUDA_CHECK(cudaGraphLaunch(b.exec, s));
+      });
+      if (nb == 1 || ms < best) best = ms, best_branches = nb;
+    }
+    b.branches = best_branches;
+    capture_batch(b);
+    FEM_CUDA_CHECK(cudaGraphLaunch(b.exec, s));  // leaves v_i = M_i u_i
     FEM_CUDA_CHECK(cudaStreamSynchronize(s));
-    b.drop_graph();
   });
 }
 
 int fem_b200_batch_info(fem_b200_batch batch, int* num_classes, int64_t* total_tiles, int64_t* total_dofs,
-                        int* graph_kernels, int* persistent_classes) {
+                        int* graph_kernels, int* persistent_classes, int* graph_branches) {
   return guarded([&] {
     require(batch && batch->d, "batch info: NULL handle");
     const BatchPlan& b = *batch->d;
@@ -490,6 +517,7 @@ int fem_b200_batch_info(fem_b200_batch batch, int* num_classes, int64_t* total_t
     if (total_dofs) *total_dofs = dofs;
     if (graph_kernels) *graph_kernels = 1 + int(b.classes.size());
     if (persistent_classes) *persistent_classes = pers;
+    if (graph_branches) *graph_branches = b.branches;
   });
 }
 

@@ -28,7 +28,17 @@ thread_local std::string g_last_error;
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 
 
-template <int P, int Q, int MINB = 1>
+// The simple kernel's register policy: no minimum of resident CTAs (ptxas'
+// own heuristic: 55 registers at P=5 where a minimum of 1 lets it take 72 and
+// lose a resident CTA); at P = 6 two resident 392-thread CTAs (83 registers,
+// 80 B of spills, against one CTA at 98 registers); at P = 8 a minimum of 1,
+// where the heuristic caps a 648-thread CTA at 40 registers and spills 1.4 KB.
+template <int P>
+constexpr int plain_min_blocks() {
+  return P >= 8 ? 1 : P == 6 ? 2 : 0;
+}
+
+template <int P, int Q, int MINB = plain_min_blocks<P>()>
 void launch_apply3(const MassPlan& p, const double* u, double* v, double* ev, cudaStream_t s) {
   using L = Mass3D<P, Q>;
   static std::atomic<uint64_t> smem_set{0};

@@ -251,7 +251,8 @@ __device__ __forceinline__ void mass3d_tile(const Mat1D<P, Q, T>& m, T* __restri
 // contributions are stored in the E-vector layout [k][i][e] (deterministic
 // mode; a transpose-map reduction follows).
 // MINB > 1 asks for MINB resident CTAs per SM (a register cap), trading a
-// little spilling for more warps to hide memory latency.  Ext adds the
+// little spilling for more warps to hide memory latency; MINB = 0 leaves the
+// register count to ptxas (fewer registers than MINB = 1 at P <= 7).  Ext adds the
 // solver's scaled gather and u^T M u reduction (apply_ext.cuh); with it the
 // kernel is persistent (tiles blockIdx.x, +gridDim.x, ...) so that each CTA
 // reduces once.  NCB > 1 runs NCB components through each phase together

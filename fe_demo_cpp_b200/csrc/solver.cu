@@ -355,11 +355,12 @@ void launch_diag(const MassPlan& p, double* diag, double* ev, cudaStream_t s) {
 }
 
 // Resident CTAs per SM the persistent CG apply asks for: the most, up to
-// kCgMaxBlocks, that leave a thread kCgMinRegs registers (P <= 5; higher
-// orders need all the registers one CTA per SM leaves).
+// kCgMaxBlocks, that leave a thread kCgMinRegs registers (P <= 5); higher
+// orders leave registers to ptxas (0), P = 8 asks for one CTA (see
+// plain_min_blocks in device.cu).
 constexpr int kCgMaxBlocks = 4, kCgMinRegs = 56;
 constexpr int cg_min_blocks(int threads, int P) {
-  if (P > 5) return 1;
+  if (P > 5) return P >= 8 ? 1 : 0;
   for (int b = kCgMaxBlocks; b > 1; --b)
     if (65536 / (b * threads) >= kCgMinRegs && b * threads <= 2048) return b;
   return 1;

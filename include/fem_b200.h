@@ -354,13 +354,14 @@ int fem_b200_batch_bind(fem_b200_batch b, const void *const *u, void *const *v, 
  * kernels launched one by one into `stream`. */
 int fem_b200_batch_apply(fem_b200_batch b, int use_graph, void *stream);
 /* Time each class's schedules (one CTA per tile; a persistent grid of
- * resident CTAs) over `reps` launches, keep the faster, and re-capture at
- * the next graph apply.  Leaves v_i = M_i u_i.  Synchronises the stream. */
+ * resident CTAs) over `reps` launches and keep the faster; then time the
+ * graph with 1, 2 and 4 parallel branches and keep the fastest capture.
+ * Leaves v_i = M_i u_i.  Synchronises the stream. */
 int fem_b200_batch_autotune(fem_b200_batch b, int reps, void *stream);
 /* Any output may be NULL: classes, tiles, sum of l_size (DoFs), kernels per
- * graph launch, classes on the persistent schedule. */
+ * graph launch, classes on the persistent schedule, parallel graph branches. */
 int fem_b200_batch_info(fem_b200_batch b, int *num_classes, int64_t *total_tiles, int64_t *total_dofs,
-                        int *graph_kernels, int *persistent_classes);
+                        int *graph_kernels, int *persistent_classes, int *graph_branches);
 int fem_b200_batch_destroy(fem_b200_batch b);
 
 /* ---- served solves (no reference counterpart) ------------------------------

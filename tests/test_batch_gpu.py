@@ -127,6 +127,7 @@ def test_graph_replay_rebind_and_autotune(fem, cuda):
         close(host(vs2[i]), host(want), TOL)
     b.autotune(reps=2)
     assert 0 <= b.info()["persistent_classes"] <= b.info()["classes"]
+    assert b.info()["graph_branches"] in (1, 2, 4)
     for v in vs2:
         v.fill_(3.0)
     b.apply()
