@@ -552,6 +552,8 @@ int fem_b200_basis_apply(fem_b200_basis b, int num_elem, int t_mode, int eval_mo
     const int64_t out_n = tr ? pn : (grad ? h.dim * qn : qn);
     require(n_u == in_n && u, "tensor_basis_apply: u has the wrong size");
     require(n_v == out_n && v, "tensor_basis_apply: v has the wrong size");
+    // dim 3: one fused pass, no scratch
+    if (basis3d_fused_apply(h, num_elem, tr, grad, u, v, s)) return;
     const int P = tr ? h.Q : h.P, Q = tr ? h.P : h.Q;  // contracted in / out sizes
     const int64_t big = h.num_comp * ipow(std::max(h.P, h.Q), h.dim) * num_elem;
     std::lock_guard<std::mutex> lock(bd.scratch_mu);

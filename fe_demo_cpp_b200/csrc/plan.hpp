@@ -279,6 +279,11 @@ void mass_build_impl(const BasisData& b, const RestrictionData& r, const double*
 std::unique_ptr<MassPlan> make_mass_plan(const std::shared_ptr<RestrictionData>& r, const BasisData& b,
                                          const double* qdata, int qf, cudaStream_t s);
 
+// Defined in basis.cu: the fused dim-3 interp / grad applies (E-vector <->
+// Q-vector, no scratch); false where no fused kernel exists for the shape.
+bool basis3d_fused_apply(const BasisData& b, int num_elem, bool transpose, bool grad, const double* u, double* v,
+                         cudaStream_t s);
+
 // Defined in solver.cu.
 struct SolveStats {
   int iterations = 0, refinements = 0;
