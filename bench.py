@@ -355,6 +355,27 @@ def run_sweep(args):
                                   "roofline_frac": abytes / (kms * 1e-3) / 1e9 / peak,
                                   "fp64_tflops": algorithmic_flops(ne, Pp, Qq, nc) / (kms * 1e-3) / 1e12}),
                       flush=True)
+            # reduced storage: FP32 (u, v, qdata) and BF16 (u, qdata; FP32 v), public applies
+            for name, uu, vv, ab in (
+                    ("fp32", u.float(), torch.empty(nc * N, dtype=torch.float32, device=dev),
+                     ne * (4 * Pp**3 + 4 * Qq**3) + 8 * nc * N),
+                    ("bf16", u.to(torch.bfloat16), torch.empty(nc * N, dtype=torch.float32, device=dev),
+                     ne * (4 * Pp**3 + 2 * Qq**3) + 6 * nc * N)):
+                fn = op.apply_f32 if name == "fp32" else op.apply_bf16
+                for _ in range(3):
+                    fn(uu, vv)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                for _ in range(args.sweep_steps):
+                    fn(uu, vv)
+                e1.record()
+                torch.cuda.synchronize()
+                ms = e0.elapsed_time(e1) / args.sweep_steps
+                print(json.dumps({"sweep": "mass_apply_storage", "storage": name, "P": Pp, "Q": Qq, "num_comp": nc,
+                                  "dofs": nc * N, "ms_per_apply": ms, "gdofs": nc * N / ms / 1e6,
+                                  "algorithmic_bytes": ab, "roofline_frac": ab / (ms * 1e-3) / 1e9 / peak}),
+                      flush=True)
+                del uu, vv
             op.set_kernel(fem.KernelVariant.auto)
             ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             ev[0].record()

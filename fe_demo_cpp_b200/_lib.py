@@ -64,6 +64,8 @@ SIGNATURES = {
     "fem_b200_mass_check": ([_p, _p], _i),
     "fem_b200_mass_diagonal": ([_p, _p, _i64, _p], _i),
     "fem_b200_mass_solve": ([_p, _p, _i64, _p, _i64, C.c_double, _i, _i, _p, _p, _p, _p], _i),
+    "fem_b200_mass_apply_f32": ([_p, _p, _i64, _p, _i64, _p], _i),
+    "fem_b200_mass_apply_bf16": ([_p, _p, _i64, _p, _i64, _p], _i),
     "fem_b200_batch_create": ([_p, _i, _i, _p], _i),
     "fem_b200_batch_bind": ([_p, _p, _p, _p], _i),
     "fem_b200_batch_apply": ([_p, _i, _p], _i),

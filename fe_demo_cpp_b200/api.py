@@ -296,6 +296,18 @@ class MassOperator(_Handle):
              C.addressof(ms), _stream(stream))
         return KernelVariant(chosen.value).name, ms.value
 
+    def apply_f32(self, u, v, stream=None):
+        """v = M u in FP32 storage and arithmetic (float32 device tensors)."""
+        _check_dev(u, "float32")
+        _check_dev(v, "float32")
+        call("fem_b200_mass_apply_f32", self.h, _ptr(u), _n(u), _ptr(v), _n(v), _stream(stream))
+
+    def apply_bf16(self, u, v, stream=None):
+        """v (float32) = M u with u (bfloat16) and qdata in BF16 storage, FP32 arithmetic."""
+        _check_dev(u, "bfloat16")
+        _check_dev(v, "float32")
+        call("fem_b200_mass_apply_bf16", self.h, _ptr(u), _n(u), _ptr(v), _n(v), _stream(stream))
+
     def diagonal(self, diag, stream=None) -> None:
         """diag (device, l_size) = the assembled diagonal of M."""
         _check_dev(diag)

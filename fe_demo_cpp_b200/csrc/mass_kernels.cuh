@@ -22,11 +22,25 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <cuda_bf16.h>
+
+#include <type_traits>
+
 #include <cstdint>
 
 #include "apply_ext.cuh"
 
 namespace fem_b200 {
+
+// A value of storage type S read as compute type T (S = T, or BF16 storage
+// of u and qdata under FP32 arithmetic).
+template <class T, class S>
+__device__ __forceinline__ T load_as(const S* p) {
+  if constexpr (std::is_same<S, __nv_bfloat16>::value)
+    return T(__bfloat162float(*p));
+  else
+    return T(__ldg(p));
+}
 
 template <int P, int Q, class T = double>
 struct Mat1D {
@@ -103,10 +117,10 @@ struct Mass3D {
 
 // One 8-element tile of the 3D fused apply (the body of mass3d_apply_kernel and
 // of the batched kernels): sa / sb are the CTA's shared buffers A and B.
-template <int P, int Q, class T, class Ext, int NCB>
+template <int P, int Q, class T, class Ext, int NCB, class S = T>
 __device__ __forceinline__ void mass3d_tile(const Mat1D<P, Q, T>& m, T* __restrict__ sa, T* __restrict__ sb,
-                                            const int* __restrict__ offs, const T* __restrict__ qd,
-                                            const T* __restrict__ u, T* __restrict__ v, T* __restrict__ ev,
+                                            const int* __restrict__ offs, const S* __restrict__ qd,
+                                            const S* __restrict__ u, T* __restrict__ v, T* __restrict__ ev,
                                             int num_elem, int num_comp_run, int64_t comp_stride,
                                             const Ext& ext, const int64_t tile, double& dsum) {
   using L = Mass3D<P, Q>;
@@ -119,9 +133,9 @@ __device__ __forceinline__ void mass3d_tile(const Mat1D<P, Q, T>& m, T* __restri
   // Prefetch: this thread's qdata row (qy, qz) = (col % Q, col / Q), all qx.
   T qv[Q];
   {
-    const T* qt = qd + tile * (int64_t(L::NQ) * E) + col * E + e;
+    const S* qt = qd + tile * (int64_t(L::NQ) * E) + col * E + e;
 #pragma unroll
-    for (int qx = 0; qx < Q; ++qx) qv[qx] = __ldg(qt + qx * (Q * Q * E));
+    for (int qx = 0; qx < Q; ++qx) qv[qx] = load_as<T>(qt + qx * (Q * Q * E));
   }
   int off[P];
   if (nodal) {
@@ -140,7 +154,7 @@ __device__ __forceinline__ void mass3d_tile(const Mat1D<P, Q, T>& m, T* __restri
         if constexpr (Ext::kScale) sc = __ldg(ext.scale + off[pz]);
 #pragma unroll
         for (int c = 0; c < NCB; ++c) {
-          x[c][pz] = __ldg(u + off[pz] + (k0 + c) * comp_stride);
+          x[c][pz] = load_as<T>(u + off[pz] + (k0 + c) * comp_stride);
           if constexpr (Ext::kScale) x[c][pz] *= sc;
         }
       }
@@ -258,10 +272,10 @@ __device__ __forceinline__ void mass3d_tile(const Mat1D<P, Q, T>& m, T* __restri
 // reduces once.  NCB > 1 runs NCB components through each phase together
 // (num_comp_run a multiple of NCB, shared memory NCB * (SA + SB)): more loads
 // in flight and a third of the barriers for a 3-component field.
-template <int P, int Q, int MINB = 1, class T = double, class Ext = ApplyPlain, int NCB = 1>
+template <int P, int Q, int MINB = 1, class T = double, class Ext = ApplyPlain, int NCB = 1, class S = T>
 __global__ void __launch_bounds__(Mass3D<P, Q>::NT, MINB) mass3d_apply_kernel(
-    const __grid_constant__ Mat1D<P, Q, T> m, const int* __restrict__ offs, const T* __restrict__ qd,
-    const T* __restrict__ u, T* __restrict__ v, T* __restrict__ ev, int num_elem, int num_comp_run,
+    const __grid_constant__ Mat1D<P, Q, T> m, const int* __restrict__ offs, const S* __restrict__ qd,
+    const S* __restrict__ u, T* __restrict__ v, T* __restrict__ ev, int num_elem, int num_comp_run,
     int64_t comp_stride, const Ext ext) {
   using L = Mass3D<P, Q>;
   constexpr int E = L::E;
@@ -276,13 +290,13 @@ __global__ void __launch_bounds__(Mass3D<P, Q>::NT, MINB) mass3d_apply_kernel(
   if constexpr (Ext::kDot) {  // persistent: one reduction per CTA
     const int64_t n_tiles = (int64_t(num_elem) + E - 1) / E;
     for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x)
-      mass3d_tile<P, Q, T, Ext, NCB>(m, sa, sb, offs, qd, u, v, ev, num_elem, num_comp_run, comp_stride, ext, tile,
+      mass3d_tile<P, Q, T, Ext, NCB, S>(m, sa, sb, offs, qd, u, v, ev, num_elem, num_comp_run, comp_stride, ext, tile,
                                      dsum);
     double dv[1] = {dsum};
     grid_sum<1>(dv, ext.part, &ext.st->ticket, [&](const double* tot) { cg_after_apply(ext.st, tot[0]); });
   } else {
-    mass3d_tile<P, Q, T, Ext, NCB>(m, sa, sb, offs, qd, u, v, ev, num_elem, num_comp_run, comp_stride, ext,
-                                   blockIdx.x, dsum);
+    mass3d_tile<P, Q, T, Ext, NCB, S>(m, sa, sb, offs, qd, u, v, ev, num_elem, num_comp_run, comp_stride, ext,
+                                      blockIdx.x, dsum);
   }
 }
 
@@ -420,10 +434,10 @@ struct Mass2D {
 };
 
 // One 32-element tile of the 2D fused apply: s1 / s3 the CTA's shared buffers.
-template <int P, int Q, class T, class Ext>
+template <int P, int Q, class T, class Ext, class S = T>
 __device__ __forceinline__ void mass2d_tile(const Mat1D<P, Q, T>& m, T* __restrict__ s1, T* __restrict__ s3,
-                                            const int* __restrict__ offs, const T* __restrict__ qd,
-                                            const T* __restrict__ u, T* __restrict__ v, T* __restrict__ ev,
+                                            const int* __restrict__ offs, const S* __restrict__ qd,
+                                            const S* __restrict__ u, T* __restrict__ v, T* __restrict__ ev,
                                             int num_elem, int num_comp_run, int64_t comp_stride,
                                             const Ext& ext, const int64_t tile, double& dsum) {
   using L = Mass2D<P, Q>;
@@ -434,9 +448,9 @@ __device__ __forceinline__ void mass2d_tile(const Mat1D<P, Q, T>& m, T* __restri
   const bool valid = eg < num_elem;
   T qv[Q];
   {
-    const T* qt = qd + tile * (int64_t(L::NQ) * E) + col * E + e;
+    const S* qt = qd + tile * (int64_t(L::NQ) * E) + col * E + e;
 #pragma unroll
-    for (int qx = 0; qx < Q; ++qx) qv[qx] = __ldg(qt + qx * (Q * E));
+    for (int qx = 0; qx < Q; ++qx) qv[qx] = load_as<T>(qt + qx * (Q * E));
   }
   int off[P];
   if (nodal) {
@@ -450,7 +464,7 @@ __device__ __forceinline__ void mass2d_tile(const Mat1D<P, Q, T>& m, T* __restri
       T x[P];
 #pragma unroll
       for (int py = 0; py < P; ++py) {
-        x[py] = __ldg(u + off[py] + ks);
+        x[py] = load_as<T>(u + off[py] + ks);
         if constexpr (Ext::kScale) x[py] *= __ldg(ext.scale + off[py]);
       }
 #pragma unroll
@@ -505,10 +519,10 @@ __device__ __forceinline__ void mass2d_tile(const Mat1D<P, Q, T>& m, T* __restri
   }
 }
 
-template <int P, int Q, class T = double, class Ext = ApplyPlain>
+template <int P, int Q, class T = double, class Ext = ApplyPlain, class S = T>
 __global__ void __launch_bounds__(Mass2D<P, Q>::NT) mass2d_apply_kernel(
-    const __grid_constant__ Mat1D<P, Q, T> m, const int* __restrict__ offs, const T* __restrict__ qd,
-    const T* __restrict__ u, T* __restrict__ v, T* __restrict__ ev, int num_elem, int num_comp_run,
+    const __grid_constant__ Mat1D<P, Q, T> m, const int* __restrict__ offs, const S* __restrict__ qd,
+    const S* __restrict__ u, T* __restrict__ v, T* __restrict__ ev, int num_elem, int num_comp_run,
     int64_t comp_stride, const Ext ext) {
   using L = Mass2D<P, Q>;
   constexpr int E = L::E;
@@ -522,12 +536,13 @@ __global__ void __launch_bounds__(Mass2D<P, Q>::NT) mass2d_apply_kernel(
   if constexpr (Ext::kDot) {  // persistent, one reduction per CTA
     const int64_t n_tiles = (int64_t(num_elem) + E - 1) / E;
     for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x)
-      mass2d_tile<P, Q, T, Ext>(m, s1, s3, offs, qd, u, v, ev, num_elem, num_comp_run, comp_stride, ext, tile, dsum);
+      mass2d_tile<P, Q, T, Ext, S>(m, s1, s3, offs, qd, u, v, ev, num_elem, num_comp_run, comp_stride, ext, tile,
+                                   dsum);
     double dv[1] = {dsum};
     grid_sum<1>(dv, ext.part, &ext.st->ticket, [&](const double* tot) { cg_after_apply(ext.st, tot[0]); });
   } else {
-    mass2d_tile<P, Q, T, Ext>(m, s1, s3, offs, qd, u, v, ev, num_elem, num_comp_run, comp_stride, ext, blockIdx.x,
-                              dsum);
+    mass2d_tile<P, Q, T, Ext, S>(m, s1, s3, offs, qd, u, v, ev, num_elem, num_comp_run, comp_stride, ext,
+                                 blockIdx.x, dsum);
   }
 }
 
@@ -597,9 +612,9 @@ __global__ void __launch_bounds__(32 * Q) mass2d_build_kernel(const __grid_const
 // dim = 1: one thread per element, everything in registers.
 // ---------------------------------------------------------------------------
 // One element of mass1d_apply_kernel (E = 128 elements per tile).
-template <int P, int Q, class T, class Ext>
+template <int P, int Q, class T, class Ext, class S = T>
 __device__ __forceinline__ void mass1d_element(const Mat1D<P, Q, T>& m, const int* __restrict__ offs,
-                                               const T* __restrict__ qd, const T* __restrict__ u,
+                                               const S* __restrict__ qd, const S* __restrict__ u,
                                                T* __restrict__ v, T* __restrict__ ev, int num_elem,
                                                int num_comp_run, int64_t comp_stride, const Ext& ext,
                                                int64_t tile, int e, int64_t eg, double& dsum) {
@@ -609,13 +624,13 @@ __device__ __forceinline__ void mass1d_element(const Mat1D<P, Q, T>& m, const in
 #pragma unroll
   for (int px = 0; px < P; ++px) off[px] = __ldg(offs + (tile * P + px) * E + e);
 #pragma unroll
-  for (int qx = 0; qx < Q; ++qx) qv[qx] = __ldg(qd + (tile * Q + qx) * E + e);
+  for (int qx = 0; qx < Q; ++qx) qv[qx] = load_as<T>(qd + (tile * Q + qx) * E + e);
   for (int k = 0; k < num_comp_run; ++k) {
     const int64_t ks = k * comp_stride;
     T x[P], r[Q];
 #pragma unroll
     for (int px = 0; px < P; ++px) {
-      x[px] = __ldg(u + off[px] + ks);
+      x[px] = load_as<T>(u + off[px] + ks);
       if constexpr (Ext::kScale) x[px] *= __ldg(ext.scale + off[px]);
     }
 #pragma unroll
@@ -639,10 +654,10 @@ __device__ __forceinline__ void mass1d_element(const Mat1D<P, Q, T>& m, const in
   }
 }
 
-template <int P, int Q, class T = double, class Ext = ApplyPlain>
+template <int P, int Q, class T = double, class Ext = ApplyPlain, class S = T>
 __global__ void __launch_bounds__(128) mass1d_apply_kernel(const __grid_constant__ Mat1D<P, Q, T> m,
-                                                          const int* __restrict__ offs, const T* __restrict__ qd,
-                                                          const T* __restrict__ u, T* __restrict__ v,
+                                                          const int* __restrict__ offs, const S* __restrict__ qd,
+                                                          const S* __restrict__ u, T* __restrict__ v,
                                                           T* __restrict__ ev, int num_elem, int num_comp_run,
                                                           int64_t comp_stride, const Ext ext) {
   constexpr int E = 128;
@@ -654,14 +669,14 @@ __global__ void __launch_bounds__(128) mass1d_apply_kernel(const __grid_constant
   if constexpr (!Ext::kDot) {
     const int64_t tile = blockIdx.x, eg = tile * E + e;
     if (eg < num_elem)
-      mass1d_element<P, Q, T, Ext>(m, offs, qd, u, v, ev, num_elem, num_comp_run, comp_stride, ext, tile, e, eg,
+      mass1d_element<P, Q, T, Ext, S>(m, offs, qd, u, v, ev, num_elem, num_comp_run, comp_stride, ext, tile, e, eg,
                                    dsum);
   } else {  // persistent, one reduction per CTA
     const int64_t n_tiles = (int64_t(num_elem) + E - 1) / E;
     for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
       const int64_t eg = tile * E + e;
       if (eg < num_elem)
-        mass1d_element<P, Q, T, Ext>(m, offs, qd, u, v, ev, num_elem, num_comp_run, comp_stride, ext, tile, e,
+        mass1d_element<P, Q, T, Ext, S>(m, offs, qd, u, v, ev, num_elem, num_comp_run, comp_stride, ext, tile, e,
                                      eg, dsum);
     }
     double dv[1] = {dsum};

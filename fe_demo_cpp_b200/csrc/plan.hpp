@@ -207,7 +207,8 @@ struct MassPlan {
   DevBuf<CgScalars> cg_st;                // device-resident solver scalars
   PinnedBuf<CgScalars> cg_host;           // their host copy
   CgScalars* cg_host_ext = nullptr;       // or a page-locked copy owned by the caller (a server slot)
-  DevBuf<float> qd_t32, dinv32, evec32;   // FP32 copies for the inner solves
+  DevBuf<float> qd_t32, dinv32, evec32;   // FP32 copies (inner solves, FP32 applies)
+  DevBuf<__nv_bfloat16> qd_t16;           // BF16 qdata (BF16-storage applies)
   DevBuf<float> f_r, f_p, f_s, f_w, f_x;  // FP32 Krylov vectors
 };
 

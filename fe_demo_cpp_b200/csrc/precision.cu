@@ -1,0 +1,187 @@
+// The mass apply in FP32 and in BF16 storage (sm_100a): the fused kernels of
+// mass_kernels.cuh instantiated with FP32 arithmetic, reading u and qdata as
+// FP32 or as BF16 (converted to FP32 at the load) and accumulating v in FP32.
+// The plan converts its tiled FP64 qdata once per storage type.  The
+// reference computes in FP64 only (src/operator.cpp:148-182); these are the
+// reduced-storage forms of the same operator.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <atomic>
+
+#include "plan.hpp"
+
+namespace fem_b200 {
+namespace {
+
+__global__ void qdata_to_f32_kernel(int64_t n, const double* __restrict__ in, float* __restrict__ out) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    out[i] = float(in[i]);
+}
+
+__global__ void qdata_to_bf16_kernel(int64_t n, const double* __restrict__ in, __nv_bfloat16* __restrict__ out) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    out[i] = __float2bfloat16_rn(float(in[i]));
+}
+
+// v += the element contributions in transpose-map order (deterministic mode)
+__global__ void csr_add_f32_kernel(int num_nodes, int num_elem, int elem_size, int num_comp, int64_t comp_stride,
+                                   const int* __restrict__ l_vec_indices, const int* __restrict__ t_offsets,
+                                   const int* __restrict__ t_indices, const float* __restrict__ ev,
+                                   float* __restrict__ v) {
+  for (int nd = blockIdx.x * blockDim.x + threadIdx.x; nd < num_nodes; nd += gridDim.x * blockDim.x) {
+    const int64_t l = l_vec_indices[nd];
+    const int t0 = t_offsets[nd], t1 = t_offsets[nd + 1];
+    for (int k = 0; k < num_comp; ++k) {
+      float sum = 0.0f;
+      for (int t = t0; t < t1; ++t) {
+        const int ti = t_indices[t];
+        const int e = ti / elem_size, i = ti - e * elem_size;
+        sum += ev[(int64_t(k) * elem_size + i) * num_elem + e];
+      }
+      v[l + k * comp_stride] += sum;
+    }
+  }
+}
+
+template <int P, int Q>
+Mat1D<P, Q, float> f32_mat(const BasisData& b) {
+  Mat1D<P, Q, float> m;
+  for (int i = 0; i < Q * P; ++i) m.B[i] = float(b.interp[i]), m.G[i] = float(b.grad[i]);
+  for (int i = 0; i < Q; ++i) m.W[i] = float(b.q_weight[i]);
+  return m;
+}
+
+// the simple kernel's register policy (as the FP64 plan's simple variant)
+template <int P>
+constexpr int lowp_min_blocks() {
+  return P >= 8 ? 1 : P == 6 ? 2 : 0;
+}
+
+template <class S>
+using LowpLauncher = void (*)(const MassPlan&, const S*, const S*, float*, float*, cudaStream_t);
+
+template <int P, int Q, class S>
+void launch_lowp(const MassPlan& p, const S* qd, const S* u, float* v, float* ev, cudaStream_t s) {
+  if (p.dim == 3) {
+    using L = Mass3D<P, Q>;
+    constexpr int smem = (L::SA + L::SB) * 4;
+    const auto kern = mass3d_apply_kernel<P, Q, lowp_min_blocks<P>(), float, ApplyPlain, 1, S>;
+    static std::atomic<uint64_t> smem_set{0};
+    set_smem(kern, smem, smem_set);
+    kern<<<unsigned(p.n_tiles), L::NT, smem, s>>>(f32_mat<P, Q>(p.basis), p.offs_t.get(), qd, u, v, ev, p.num_elem,
+                                                  p.comp_run, p.comp_stride, ApplyPlain{});
+  } else if (p.dim == 2) {
+    using L = Mass2D<P, Q>;
+    constexpr int smem = (L::S1 + L::S3) * 4;
+    const auto kern = mass2d_apply_kernel<P, Q, float, ApplyPlain, S>;
+    static std::atomic<uint64_t> smem_set{0};
+    set_smem(kern, smem, smem_set);
+    kern<<<unsigned(p.n_tiles), L::NT, smem, s>>>(f32_mat<P, Q>(p.basis), p.offs_t.get(), qd, u, v, ev, p.num_elem,
+                                                  p.comp_run, p.comp_stride, ApplyPlain{});
+  } else {
+    mass1d_apply_kernel<P, Q, float, ApplyPlain, S><<<unsigned(p.n_tiles), 128, 0, s>>>(
+        f32_mat<P, Q>(p.basis), p.offs_t.get(), qd, u, v, ev, p.num_elem, p.comp_run, p.comp_stride, ApplyPlain{});
+  }
+  FEM_LAUNCH_CHECK();
+}
+
+constexpr int kMinP = 2, kMaxP = 8, kQSpan = 3;
+
+struct LowpDispatch {
+  LowpLauncher<float> f32[kMaxP + 1][kQSpan] = {};
+  LowpLauncher<__nv_bfloat16> bf16[kMaxP + 1][kQSpan] = {};
+};
+
+template <int P, int DQ>
+struct LowpTable {
+  static void fill(LowpDispatch& d) {
+    d.f32[P][DQ] = launch_lowp<P, P + DQ, float>;
+    d.bf16[P][DQ] = launch_lowp<P, P + DQ, __nv_bfloat16>;
+    if constexpr (DQ + 1 < kQSpan)
+      LowpTable<P, DQ + 1>::fill(d);
+    else if constexpr (P + 1 <= kMaxP)
+      LowpTable<P + 1, 0>::fill(d);
+  }
+};
+
+const LowpDispatch& lowp_dispatch() {
+  static const LowpDispatch d = [] {
+    LowpDispatch t;
+    LowpTable<kMinP, 0>::fill(t);
+    return t;
+  }();
+  return d;
+}
+
+// v = M u with u, qdata in S and v in FP32
+template <class S>
+void lowp_apply(MassPlan& p, const S* u, float* v, cudaStream_t s) {
+  const size_t nq = p.qd_t.size();
+  const S* qd = nullptr;
+  if constexpr (std::is_same<S, float>::value) {
+    if (p.qd_t32.size() != nq) {
+      p.qd_t32.alloc(nq);
+      qdata_to_f32_kernel<<<grid_for(int64_t(nq), 256), 256, 0, s>>>(int64_t(nq), p.qd_t.get(), p.qd_t32.get());
+      FEM_LAUNCH_CHECK();
+    }
+    qd = p.qd_t32.get();
+  } else {
+    if (p.qd_t16.size() != nq) {
+      p.qd_t16.alloc(nq);
+      qdata_to_bf16_kernel<<<grid_for(int64_t(nq), 256), 256, 0, s>>>(int64_t(nq), p.qd_t.get(), p.qd_t16.get());
+      FEM_LAUNCH_CHECK();
+    }
+    qd = p.qd_t16.get();
+  }
+  FEM_CUDA_CHECK(cudaMemsetAsync(v, 0, size_t(p.l_size) * sizeof(float), s));
+  const LowpDispatch& d = lowp_dispatch();
+  LowpLauncher<S> launch = nullptr;
+  if constexpr (std::is_same<S, float>::value)
+    launch = d.f32[p.P][p.Q - p.P];
+  else
+    launch = d.bf16[p.P][p.Q - p.P];
+  if (p.scatter_mode == FEM_B200_SCATTER_ATOMIC) {
+    launch(p, qd, u, v, nullptr, s);
+    return;
+  }
+  if (p.evec32.size() != p.evec.size()) p.evec32.alloc(p.evec.size());
+  const RestrictionData& r = *p.r;
+  launch(p, qd, u, nullptr, p.evec32.get(), s);
+  csr_add_f32_kernel<<<grid_for(r.num_nodes, 256), 256, 0, s>>>(r.num_nodes, p.num_elem, p.es, p.comp_run,
+                                                                p.comp_stride, r.l_vec_indices.get(),
+                                                                r.t_offsets.get(), r.t_indices.get(),
+                                                                p.evec32.get(), v);
+  FEM_LAUNCH_CHECK();
+}
+
+}  // namespace
+}  // namespace fem_b200
+
+using namespace fem_b200;
+
+extern "C" {
+
+int fem_b200_mass_apply_f32(fem_b200_mass op, const float* u, int64_t n_u, float* v, int64_t n_v, void* stream) {
+  return guarded([&] {
+    require(op && op->d, "operator_apply: NULL handle");
+    MassPlan& p = *op->d;
+    require(n_u == p.l_size && u, "operator_apply: input vector size does not match active_in_l_size");
+    require(n_v == p.l_size && v, "operator_apply: output vector size does not match active_out_l_size");
+    DeviceGuard g(p.device);
+    lowp_apply<float>(p, u, v, as_stream(stream));
+  });
+}
+
+int fem_b200_mass_apply_bf16(fem_b200_mass op, const void* u, int64_t n_u, float* v, int64_t n_v, void* stream) {
+  return guarded([&] {
+    require(op && op->d, "operator_apply: NULL handle");
+    MassPlan& p = *op->d;
+    require(n_u == p.l_size && u, "operator_apply: input vector size does not match active_in_l_size");
+    require(n_v == p.l_size && v, "operator_apply: output vector size does not match active_out_l_size");
+    DeviceGuard g(p.device);
+    lowp_apply<__nv_bfloat16>(p, static_cast<const __nv_bfloat16*>(u), v, as_stream(stream));
+  });
+}
+
+}  // extern "C"

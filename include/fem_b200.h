@@ -420,6 +420,15 @@ int fem_b200_server_stats(fem_b200_server s, int64_t *submitted, int64_t *comple
 /* Finishes every queued request, then stops the workers. */
 int fem_b200_server_destroy(fem_b200_server s);
 
+/* operator_apply in reduced storage (src/operator.cpp:148-182 is FP64 only):
+ * _f32: u, v and qdata in FP32 (qdata converted once from the plan's FP64
+ * copy), FP32 arithmetic; _bf16: u and qdata in BF16 (bfloat16 bit patterns,
+ * 2 bytes an entry), FP32 arithmetic and FP32 v.  v is overwritten; both
+ * scatter modes; device pointers, `stream` order. */
+int fem_b200_mass_apply_f32(fem_b200_mass op, const float *u, int64_t n_u, float *v, int64_t n_v, void *stream);
+int fem_b200_mass_apply_bf16(fem_b200_mass op, const void *u_bf16, int64_t n_u, float *v, int64_t n_v,
+                             void *stream);
+
 /* Synchronise `stream` and report a device-side failure of the plan's kernels
  * (a bounded wait that ran out) as FEM_B200_ERROR_CUDA.  fem_b200_mass_apply_host
  * does this check itself. */
