@@ -46,6 +46,7 @@ class KernelVariant(IntEnum):
     paired = 3
     prefetch = 4
     occupancy = 5
+    narrow = 6
 
 
 class QF(IntEnum):

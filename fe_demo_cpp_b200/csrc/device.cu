@@ -18,6 +18,7 @@
 #include "mass_kernels.cuh"
 #include "mass_pipe.cuh"
 #include "mass_x2.cuh"
+#include "mass_narrow.cuh"
 #include "mass_prefetch.cuh"
 #include "plan.hpp"
 #include "restriction_kernels.cuh"
@@ -92,6 +93,21 @@ void launch_apply3_x2(const MassPlan& p, const double* u, double* v, double* ev,
   FEM_LAUNCH_CHECK();
 }
 
+// Half-tile CTAs (4 elements): at P = 8 no register cap (one CTA per SM,
+// no spills: 1.5x the one-tile kernel there), below two resident CTAs
+// (P = 7: 128 registers, P = 6: 96).
+template <int P, int Q>
+void launch_apply3_narrow(const MassPlan& p, const double* u, double* v, double* ev, cudaStream_t s) {
+  using L = Narrow3D<P, Q>;
+  constexpr int minb = P >= 8 ? 0 : 2;
+  const auto kern = mass3d_apply_narrow_kernel<P, Q, minb>;
+  static std::atomic<uint64_t> smem_set{0};
+  set_smem(kern, L::SMEM, smem_set);
+  kern<<<unsigned(2 * p.n_tiles), L::NT, L::SMEM, s>>>(make_mat<P, Q>(p.basis), p.offs_t.get(), p.qd_t.get(), u,
+                                                       v, ev, p.num_elem, p.comp_run, p.comp_stride);
+  FEM_LAUNCH_CHECK();
+}
+
 template <int P, int Q>
 void launch_apply2(const MassPlan& p, const double* u, double* v, double* ev, cudaStream_t s) {
   using L = Mass2D<P, Q>;
@@ -146,7 +162,7 @@ template <int P, int DQ>
 struct Table {
   static void fill(ApplyLauncher (*ap)[kMaxP + 1][kQSpan], BuildLauncher (*bd)[kMaxP + 1][kQSpan],
                    ApplyLauncher (*pp)[kQSpan], ApplyLauncher (*xx)[kQSpan], ApplyLauncher (*pf)[kQSpan],
-                   ApplyLauncher (*oc)[kQSpan]) {
+                   ApplyLauncher (*oc)[kQSpan], ApplyLauncher (*nw)[kQSpan]) {
     constexpr int Q = P + DQ;
     ap[0][P][DQ] = launch_apply1<P, Q>;
     ap[1][P][DQ] = launch_apply2<P, Q>;
@@ -155,13 +171,14 @@ struct Table {
     if constexpr (Mass3DX2<P, Q>::SMEM <= kMaxSmemPerCta && Mass3DX2<P, Q>::NT <= 1024) xx[P][DQ] = launch_apply3_x2<P, Q>;
     if constexpr (Prefetch3D<P, Q>::SMEM <= kMaxSmemPerCta) pf[P][DQ] = launch_apply3_pf<P, Q>;
     if constexpr (Mass3D<P, Q>::MINB_OCC > 1) oc[P][DQ] = launch_apply3<P, Q, Mass3D<P, Q>::MINB_OCC>;
+    if constexpr (Narrow3D<P, Q>::SMEM <= kMaxSmemPerCta) nw[P][DQ] = launch_apply3_narrow<P, Q>;
     bd[0][P][DQ] = launch_build1<P, Q>;
     bd[1][P][DQ] = launch_build2<P, Q>;
     bd[2][P][DQ] = launch_build3<P, Q>;
     if constexpr (DQ + 1 < kQSpan)
-      Table<P, DQ + 1>::fill(ap, bd, pp, xx, pf, oc);
+      Table<P, DQ + 1>::fill(ap, bd, pp, xx, pf, oc, nw);
     else if constexpr (P + 1 <= kMaxP)
-      Table<P + 1, 0>::fill(ap, bd, pp, xx, pf, oc);
+      Table<P + 1, 0>::fill(ap, bd, pp, xx, pf, oc, nw);
   }
 };
 
@@ -172,7 +189,8 @@ struct Dispatch {
   ApplyLauncher apply3_x2[kMaxP + 1][kQSpan] = {};
   ApplyLauncher apply3_pf[kMaxP + 1][kQSpan] = {};
   ApplyLauncher apply3_occ[kMaxP + 1][kQSpan] = {};
-  Dispatch() { Table<kMinP, 0>::fill(apply, build, apply3_pipe, apply3_x2, apply3_pf, apply3_occ); }
+  ApplyLauncher apply3_nw[kMaxP + 1][kQSpan] = {};
+  Dispatch() { Table<kMinP, 0>::fill(apply, build, apply3_pipe, apply3_x2, apply3_pf, apply3_occ, apply3_nw); }
 };
 
 const Dispatch& dispatch() {
@@ -208,6 +226,7 @@ ApplyLauncher variant_launcher(const MassPlan& p, int variant) {
     case FEM_B200_KERNEL_PAIRED: return p.launch_x2;
     case FEM_B200_KERNEL_PREFETCH: return p.launch_pf;
     case FEM_B200_KERNEL_OCCUPANCY: return p.launch_occ;
+    case FEM_B200_KERNEL_NARROW: return p.launch_nw;
     default: return nullptr;
   }
 }
@@ -916,6 +935,7 @@ std::unique_ptr<MassPlan> make_mass_plan(const std::shared_ptr<RestrictionData>&
   p->launch_x2 = b.dim == 3 ? dispatch().apply3_x2[b.P][b.Q - b.P] : nullptr;
   p->launch_pf = b.dim == 3 ? dispatch().apply3_pf[b.P][b.Q - b.P] : nullptr;
   p->launch_occ = b.dim == 3 ? dispatch().apply3_occ[b.P][b.Q - b.P] : nullptr;
+  p->launch_nw = b.dim == 3 ? dispatch().apply3_nw[b.P][b.Q - b.P] : nullptr;
   p->launch = auto_kernel(*p);
   FEM_CUDA_CHECK(cudaStreamSynchronize(s));
   return p;
@@ -996,7 +1016,7 @@ int fem_b200_mass_autotune(fem_b200_mass op, const double* u, int64_t n_u, doubl
     int best = FEM_B200_KERNEL_SIMPLE;
     float best_t = -1.0f;
     try {
-      for (int variant = FEM_B200_KERNEL_SIMPLE; variant <= FEM_B200_KERNEL_OCCUPANCY; ++variant) {
+      for (int variant = FEM_B200_KERNEL_SIMPLE; variant <= FEM_B200_KERNEL_NARROW; ++variant) {
         ApplyLauncher l = variant_launcher(p, variant);
         if (!l) continue;
         p.launch = l;
@@ -1044,7 +1064,9 @@ int fem_b200_mass_set_kernel(fem_b200_mass op, int variant) {
   return guarded([&] {
     require(op && op->d, "operator kernel: NULL handle");
     MassPlan& p = *op->d;
-    require(variant >= FEM_B200_KERNEL_AUTO && variant <= FEM_B200_KERNEL_OCCUPANCY, "operator kernel: unknown variant");
+    require(variant >= FEM_B200_KERNEL_AUTO && variant <= FEM_B200_KERNEL_NARROW, "operator kernel: unknown variant");
+    if (variant == FEM_B200_KERNEL_NARROW && !p.launch_nw)
+      throw unsupported_error("operator kernel: no half-tile kernel for " + shape_str(p.dim, p.P, p.Q));
     if (variant == FEM_B200_KERNEL_OCCUPANCY && !p.launch_occ)
       throw unsupported_error("operator kernel: no register-capped kernel for " + shape_str(p.dim, p.P, p.Q));
     if (variant == FEM_B200_KERNEL_PREFETCH && !p.launch_pf)
@@ -1060,6 +1082,7 @@ int fem_b200_mass_set_kernel(fem_b200_mass op, int variant) {
       case FEM_B200_KERNEL_PAIRED: p.launch = p.launch_x2; break;
       case FEM_B200_KERNEL_PREFETCH: p.launch = p.launch_pf; break;
       case FEM_B200_KERNEL_OCCUPANCY: p.launch = p.launch_occ; break;
+      case FEM_B200_KERNEL_NARROW: p.launch = p.launch_nw; break;
       default: p.launch = auto_kernel(p);
     }
   });
@@ -1076,6 +1099,7 @@ int fem_b200_mass_info(fem_b200_mass op, int* launches_per_apply, int* tile_elem
                         : p.launch == p.launch_pipe ? FEM_B200_KERNEL_PIPELINED
                         : p.launch == p.launch_pf   ? FEM_B200_KERNEL_PREFETCH
                         : p.launch == p.launch_occ  ? FEM_B200_KERNEL_OCCUPANCY
+                        : p.launch == p.launch_nw   ? FEM_B200_KERNEL_NARROW
                                                     : FEM_B200_KERNEL_SIMPLE;
     if (tile_elems) *tile_elems = p.tile_e;
     if (device_bytes)

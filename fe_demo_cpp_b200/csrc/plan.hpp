@@ -199,6 +199,7 @@ struct MassPlan {
   ApplyLauncher launch_x2 = nullptr;    // two elements per thread (dim 3)
   ApplyLauncher launch_pf = nullptr;    // persistent, prefetching (dim 3)
   ApplyLauncher launch_occ = nullptr;   // one-tile CTAs, register-capped for occupancy (dim 3)
+  ApplyLauncher launch_nw = nullptr;    // half-tile CTAs (4 elements), for high order (dim 3)
   int variant = FEM_B200_KERNEL_AUTO;
   // solver state (solver.cu), allocated by the first solve
   DevBuf<double> diag, dinv;              // assembled diagonal and its inverse

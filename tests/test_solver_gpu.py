@@ -127,7 +127,7 @@ def test_fp32_refinement_reaches_fp64_accuracy(fem, cuda, orc, dim, shape, P, Q,
 
 
 @pytest.mark.parametrize("scatter", [0, 1], ids=["atomic", "deterministic"])
-@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5])
+@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5, 6])
 def test_solve_with_every_kernel_variant(fem, cuda, orc, scatter, variant):
     """The FP64 solve runs the plan's selected apply kernel; the FP32 inner
     apply is the simple kernel in every variant."""
