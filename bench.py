@@ -276,7 +276,7 @@ def run_b200(args, rank, world, local_rank):
                    "dofs": N, "elements": ne, "scatter": "atomic", "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (3.3 GB per apply); no flush",
                    "kernel": "mass3d_apply_{}kernel<{},{}>".format(
-                       {"pipelined": "pipe_", "paired": "x2_", "prefetch": "prefetch_", "occupancy": "occ_", "narrow": "narrow_"}.get(info["kernel"], ""), P, Q),
+                       {"pipelined": "pipe_", "paired": "x2_", "prefetch": "prefetch_", "occupancy": "occ_", "narrow": "narrow_", "element": "element_"}.get(info["kernel"], ""), P, Q),
                    "kernel_variant": info["kernel"], "autotuned": tuned is not None, "kernel_ms": t_kern,
                    "algorithmic_bytes_per_apply": abytes,
                    "algorithmic_flops_per_apply": algorithmic_flops(ne, P, Q)},
@@ -719,7 +719,7 @@ def main():
     ap.add_argument("--cpu-sample-s", type=float, default=12.0, help="approximate CPU seconds of the baseline")
     ap.add_argument("--shape", default=None, help="elements per direction nx,ny,nz (default 100,100,100)")
     ap.add_argument("--P", type=int, default=None, help="nodes per direction (Q = P+1)")
-    ap.add_argument("--kernel", choices=["auto", "simple", "pipelined", "paired", "prefetch", "occupancy", "narrow"], default="auto")
+    ap.add_argument("--kernel", choices=["auto", "simple", "pipelined", "paired", "prefetch", "occupancy", "narrow", "element"], default="auto")
     ap.add_argument("--sweep", action="store_true", help="order sweep P=2..8, num_comp 1 and 3 (extra lines)")
     ap.add_argument("--sweep-P", default="2,3,4,5,6,7,8")
     ap.add_argument("--sweep-steps", type=int, default=20)

@@ -47,6 +47,7 @@ class KernelVariant(IntEnum):
     prefetch = 4
     occupancy = 5
     narrow = 6
+    element = 7
 
 
 class QF(IntEnum):

@@ -18,6 +18,7 @@
 #include "mass_kernels.cuh"
 #include "mass_pipe.cuh"
 #include "mass_x2.cuh"
+#include "mass_element.cuh"
 #include "mass_narrow.cuh"
 #include "mass_prefetch.cuh"
 #include "plan.hpp"
@@ -108,6 +109,15 @@ void launch_apply3_narrow(const MassPlan& p, const double* u, double* v, double*
   FEM_LAUNCH_CHECK();
 }
 
+// One element per thread (P <= 3): 128-thread CTAs over the plan's elements.
+template <int P, int Q>
+void launch_apply3_element(const MassPlan& p, const double* u, double* v, double* ev, cudaStream_t s) {
+  const unsigned grid = unsigned((p.n_tiles * 8 + 127) / 128);
+  mass3d_apply_element_kernel<P, Q><<<grid, 128, 0, s>>>(make_mat<P, Q>(p.basis), p.offs_t.get(), p.qd_t.get(), u,
+                                                          v, ev, p.num_elem, p.comp_run, p.comp_stride);
+  FEM_LAUNCH_CHECK();
+}
+
 template <int P, int Q>
 void launch_apply2(const MassPlan& p, const double* u, double* v, double* ev, cudaStream_t s) {
   using L = Mass2D<P, Q>;
@@ -162,7 +172,7 @@ template <int P, int DQ>
 struct Table {
   static void fill(ApplyLauncher (*ap)[kMaxP + 1][kQSpan], BuildLauncher (*bd)[kMaxP + 1][kQSpan],
                    ApplyLauncher (*pp)[kQSpan], ApplyLauncher (*xx)[kQSpan], ApplyLauncher (*pf)[kQSpan],
-                   ApplyLauncher (*oc)[kQSpan], ApplyLauncher (*nw)[kQSpan]) {
+                   ApplyLauncher (*oc)[kQSpan], ApplyLauncher (*nw)[kQSpan], ApplyLauncher (*el)[kQSpan]) {
     constexpr int Q = P + DQ;
     ap[0][P][DQ] = launch_apply1<P, Q>;
     ap[1][P][DQ] = launch_apply2<P, Q>;
@@ -172,13 +182,14 @@ struct Table {
     if constexpr (Prefetch3D<P, Q>::SMEM <= kMaxSmemPerCta) pf[P][DQ] = launch_apply3_pf<P, Q>;
     if constexpr (Mass3D<P, Q>::MINB_OCC > 1) oc[P][DQ] = launch_apply3<P, Q, Mass3D<P, Q>::MINB_OCC>;
     if constexpr (Narrow3D<P, Q>::SMEM <= kMaxSmemPerCta) nw[P][DQ] = launch_apply3_narrow<P, Q>;
+    if constexpr (P <= 3) el[P][DQ] = launch_apply3_element<P, Q>;  // registers: 86 (P=2), 250 (P=3)
     bd[0][P][DQ] = launch_build1<P, Q>;
     bd[1][P][DQ] = launch_build2<P, Q>;
     bd[2][P][DQ] = launch_build3<P, Q>;
     if constexpr (DQ + 1 < kQSpan)
-      Table<P, DQ + 1>::fill(ap, bd, pp, xx, pf, oc, nw);
+      Table<P, DQ + 1>::fill(ap, bd, pp, xx, pf, oc, nw, el);
     else if constexpr (P + 1 <= kMaxP)
-      Table<P + 1, 0>::fill(ap, bd, pp, xx, pf, oc, nw);
+      Table<P + 1, 0>::fill(ap, bd, pp, xx, pf, oc, nw, el);
   }
 };
 
@@ -190,7 +201,10 @@ struct Dispatch {
   ApplyLauncher apply3_pf[kMaxP + 1][kQSpan] = {};
   ApplyLauncher apply3_occ[kMaxP + 1][kQSpan] = {};
   ApplyLauncher apply3_nw[kMaxP + 1][kQSpan] = {};
-  Dispatch() { Table<kMinP, 0>::fill(apply, build, apply3_pipe, apply3_x2, apply3_pf, apply3_occ, apply3_nw); }
+  ApplyLauncher apply3_el[kMaxP + 1][kQSpan] = {};
+  Dispatch() {
+    Table<kMinP, 0>::fill(apply, build, apply3_pipe, apply3_x2, apply3_pf, apply3_occ, apply3_nw, apply3_el);
+  }
 };
 
 const Dispatch& dispatch() {
@@ -227,6 +241,7 @@ ApplyLauncher variant_launcher(const MassPlan& p, int variant) {
     case FEM_B200_KERNEL_PREFETCH: return p.launch_pf;
     case FEM_B200_KERNEL_OCCUPANCY: return p.launch_occ;
     case FEM_B200_KERNEL_NARROW: return p.launch_nw;
+    case FEM_B200_KERNEL_ELEMENT: return p.launch_el;
     default: return nullptr;
   }
 }
@@ -936,6 +951,7 @@ std::unique_ptr<MassPlan> make_mass_plan(const std::shared_ptr<RestrictionData>&
   p->launch_pf = b.dim == 3 ? dispatch().apply3_pf[b.P][b.Q - b.P] : nullptr;
   p->launch_occ = b.dim == 3 ? dispatch().apply3_occ[b.P][b.Q - b.P] : nullptr;
   p->launch_nw = b.dim == 3 ? dispatch().apply3_nw[b.P][b.Q - b.P] : nullptr;
+  p->launch_el = b.dim == 3 ? dispatch().apply3_el[b.P][b.Q - b.P] : nullptr;
   p->launch = auto_kernel(*p);
   FEM_CUDA_CHECK(cudaStreamSynchronize(s));
   return p;
@@ -1016,7 +1032,7 @@ int fem_b200_mass_autotune(fem_b200_mass op, const double* u, int64_t n_u, doubl
     int best = FEM_B200_KERNEL_SIMPLE;
     float best_t = -1.0f;
     try {
-      for (int variant = FEM_B200_KERNEL_SIMPLE; variant <= FEM_B200_KERNEL_NARROW; ++variant) {
+      for (int variant = FEM_B200_KERNEL_SIMPLE; variant <= FEM_B200_KERNEL_ELEMENT; ++variant) {
         ApplyLauncher l = variant_launcher(p, variant);
         if (!l) continue;
         p.launch = l;
@@ -1064,7 +1080,9 @@ int fem_b200_mass_set_kernel(fem_b200_mass op, int variant) {
   return guarded([&] {
     require(op && op->d, "operator kernel: NULL handle");
     MassPlan& p = *op->d;
-    require(variant >= FEM_B200_KERNEL_AUTO && variant <= FEM_B200_KERNEL_NARROW, "operator kernel: unknown variant");
+    require(variant >= FEM_B200_KERNEL_AUTO && variant <= FEM_B200_KERNEL_ELEMENT, "operator kernel: unknown variant");
+    if (variant == FEM_B200_KERNEL_ELEMENT && !p.launch_el)
+      throw unsupported_error("operator kernel: no element-per-thread kernel for " + shape_str(p.dim, p.P, p.Q));
     if (variant == FEM_B200_KERNEL_NARROW && !p.launch_nw)
       throw unsupported_error("operator kernel: no half-tile kernel for " + shape_str(p.dim, p.P, p.Q));
     if (variant == FEM_B200_KERNEL_OCCUPANCY && !p.launch_occ)
@@ -1083,6 +1101,7 @@ int fem_b200_mass_set_kernel(fem_b200_mass op, int variant) {
       case FEM_B200_KERNEL_PREFETCH: p.launch = p.launch_pf; break;
       case FEM_B200_KERNEL_OCCUPANCY: p.launch = p.launch_occ; break;
       case FEM_B200_KERNEL_NARROW: p.launch = p.launch_nw; break;
+      case FEM_B200_KERNEL_ELEMENT: p.launch = p.launch_el; break;
       default: p.launch = auto_kernel(p);
     }
   });
@@ -1100,6 +1119,7 @@ int fem_b200_mass_info(fem_b200_mass op, int* launches_per_apply, int* tile_elem
                         : p.launch == p.launch_pf   ? FEM_B200_KERNEL_PREFETCH
                         : p.launch == p.launch_occ  ? FEM_B200_KERNEL_OCCUPANCY
                         : p.launch == p.launch_nw   ? FEM_B200_KERNEL_NARROW
+                        : p.launch == p.launch_el   ? FEM_B200_KERNEL_ELEMENT
                                                     : FEM_B200_KERNEL_SIMPLE;
     if (tile_elems) *tile_elems = p.tile_e;
     if (device_bytes)

@@ -200,6 +200,7 @@ struct MassPlan {
   ApplyLauncher launch_pf = nullptr;    // persistent, prefetching (dim 3)
   ApplyLauncher launch_occ = nullptr;   // one-tile CTAs, register-capped for occupancy (dim 3)
   ApplyLauncher launch_nw = nullptr;    // half-tile CTAs (4 elements), for high order (dim 3)
+  ApplyLauncher launch_el = nullptr;    // one element per thread, no shared memory (dim 3, P = 2)
   int variant = FEM_B200_KERNEL_AUTO;
   // solver state (solver.cu), allocated by the first solve
   DevBuf<double> diag, dinv;              // assembled diagonal and its inverse

@@ -65,6 +65,7 @@ extern "C" {
 #define FEM_B200_KERNEL_PREFETCH 4  /* persistent CTAs, qdata bulk-copied two tiles ahead, offsets/u one ahead */
 #define FEM_B200_KERNEL_OCCUPANCY 5 /* as SIMPLE, registers capped for up to 5 resident CTAs per SM */
 #define FEM_B200_KERNEL_NARROW 6    /* half-tile CTAs of 4 elements: twice the registers a thread (high order) */
+#define FEM_B200_KERNEL_ELEMENT 7   /* one element per thread in registers, no shared memory (P <= 3) */
 
 typedef struct fem_b200_restriction_s *fem_b200_restriction;
 typedef struct fem_b200_basis_s *fem_b200_basis;
