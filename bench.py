@@ -709,6 +709,77 @@ def run_serve(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# the restriction stages against the reference's own CUDA kernels
+# (src/cuda/cuda-elem-restriction.cu built for sm_100a, oracle/_ref) on the
+# bench mesh: gather, atomic and deterministic scatter (extra lines)
+# ---------------------------------------------------------------------------
+def run_restriction(args):
+    import torch
+    import fe_demo_cpp_b200 as fem
+    import oracle
+    from fe_demo_cpp_b200.build import build
+    from fe_demo_cpp_b200.mesh import box_mesh
+
+    build()
+    if not oracle.refcuda_available():
+        print(json.dumps({"restriction": "reference-cuda", "unavailable": "oracle/_ref/libfemrefcuda.so not built"}))
+        return 0
+    dev = torch.device("cuda", 0)
+    mesh = box_mesh(SHAPE, P, seed=SEED)
+    N, ne, es = mesh.num_nodes, mesh.num_elem, P**3
+    n_e = ne * es
+    peak, _ = measured_peaks()
+    rng = np.random.default_rng([SEED, 9])
+    l_host = rng.uniform(-1, 1, N)
+    e_host = rng.uniform(-1, 1, n_e)
+    K = args.restriction_steps
+    results = {}
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(K):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / K
+
+    # algorithmic bytes: offsets, the L-vector once, the E-vector once (scatter: L read + written)
+    bytes_gather = 4 * n_e + 8 * N + 8 * n_e
+    bytes_scatter = 4 * n_e + 8 * n_e + 16 * N
+    l_dev = torch.from_numpy(l_host).to(dev)
+    e_dev = torch.from_numpy(e_host).to(dev)
+    for det in (False, True):
+        ours = fem.Restriction(ne, es, 1, N, N, mesh.offsets, 1 if det else 0)
+        ref = oracle.RefCudaRestriction(ne, es, 1, N, N, mesh.offsets, det)
+        ref.set_l(l_host)
+        ref.set_e(e_host)
+        e_out = torch.empty(n_e, dtype=torch.float64, device=dev)
+        l_out = torch.zeros(N, dtype=torch.float64, device=dev)
+        if not det:
+            results[("gather", "b200")] = timed(lambda: ours.apply(0, l_dev, e_out))
+            results[("gather", "reference-cuda")] = timed(lambda: ref.apply(False))
+            assert np.array_equal(e_out.cpu().numpy(), ref.get_e())  # parity guard
+        mode = "scatter_deterministic" if det else "scatter_atomic"
+        results[(mode, "b200")] = timed(lambda: ours.apply(1, e_dev, l_out))
+        results[(mode, "reference-cuda")] = timed(lambda: ref.apply(True))
+        ref.close()
+        del ours, e_out, l_out
+    for (mode, impl), ms in results.items():
+        ab = bytes_gather if mode == "gather" else bytes_scatter
+        other = results[(mode, "reference-cuda" if impl == "b200" else "b200")]
+        print(json.dumps({"restriction": mode, "impl": impl, "ms": ms, "algorithmic_bytes": ab,
+                          "achieved_gbs": ab / (ms * 1e-3) / 1e9, "roofline_frac": ab / (ms * 1e-3) / 1e9 / peak,
+                          "speedup_vs_other": other / ms,
+                          "config": {"mesh": "x".join(map(str, SHAPE)), "P": P, "num_comp": 1, "dofs": N,
+                                     "e_size": n_e}}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -737,7 +808,12 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=64)
     ap.add_argument("--serve-slots", type=int, default=8)
     ap.add_argument("--serve-budget-gb", type=float, default=120.0)
+    ap.add_argument("--restriction", action="store_true",
+                    help="restriction stages vs the reference's CUDA kernels (extra lines)")
+    ap.add_argument("--restriction-steps", type=int, default=20)
     args = ap.parse_args()
+    if args.restriction:
+        return run_restriction(args)
     if args.serve:
         return run_serve(args)
     if args.batch:

@@ -481,9 +481,8 @@ int fem_b200_restriction_apply(fem_b200_restriction r, int t_mode, const double*
         offset_tile_kernel<1><<<grid, block, 0, s>>>(d.offsets.get(), d.num_elem, d.elem_size, d.num_comp,
                                                      d.comp_stride, in, out);
     } else {
-      csr_scatter_kernel<<<grid_for(d.num_nodes, 256), 256, 0, s>>>(
-          d.num_nodes, d.num_elem, d.elem_size, d.num_comp, d.comp_stride, d.l_vec_indices.get(), d.t_offsets.get(),
-          d.t_indices.get(), in, out);
+      launch_csr_scatter(d.num_nodes, d.num_elem, d.elem_size, d.num_comp, d.comp_stride, d.l_vec_indices.get(),
+                         d.t_offsets.get(), d.t_indices.get(), in, out, s);
     }
     FEM_LAUNCH_CHECK();
   });
@@ -765,8 +764,8 @@ int fem_b200_transpose_scatter_add(int num_nodes, int num_elem, int elem_size, i
     require(num_nodes >= 0 && num_elem > 0 && elem_size > 0 && num_comp > 0, "transpose scatter: bad sizes");
     if (num_nodes == 0) return;
     require(l_vec_indices && t_offsets && t_indices && e_in && l_out, "transpose scatter: NULL array");
-    csr_scatter_kernel<<<grid_for(num_nodes, 256), 256, 0, as_stream(stream)>>>(
-        num_nodes, num_elem, elem_size, num_comp, comp_stride, l_vec_indices, t_offsets, t_indices, e_in, l_out);
+    launch_csr_scatter(num_nodes, num_elem, elem_size, num_comp, comp_stride, l_vec_indices, t_offsets, t_indices,
+                       e_in, l_out, as_stream(stream));
     FEM_LAUNCH_CHECK();
   });
 }
@@ -965,9 +964,8 @@ void mass_apply_impl(MassPlan& p, const double* u, double* v, bool zero, cudaStr
   }
   const RestrictionData& r = *p.r;
   p.launch(p, u, v, p.evec.get(), s);
-  csr_scatter_kernel<<<grid_for(r.num_nodes, 256), 256, 0, s>>>(r.num_nodes, p.num_elem, p.es, p.comp_run,
-                                                                p.comp_stride, r.l_vec_indices.get(),
-                                                                r.t_offsets.get(), r.t_indices.get(), p.evec.get(), v);
+  launch_csr_scatter(r.num_nodes, p.num_elem, p.es, p.comp_run, p.comp_stride, r.l_vec_indices.get(),
+                     r.t_offsets.get(), r.t_indices.get(), p.evec.get(), v, s);
   FEM_LAUNCH_CHECK();
 }
 }  // namespace fem_b200

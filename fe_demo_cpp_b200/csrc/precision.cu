@@ -10,6 +10,7 @@
 #include <atomic>
 
 #include "plan.hpp"
+#include "transpose_scatter.cuh"
 
 namespace fem_b200 {
 namespace {
@@ -22,26 +23,6 @@ __global__ void qdata_to_f32_kernel(int64_t n, const double* __restrict__ in, fl
 __global__ void qdata_to_bf16_kernel(int64_t n, const double* __restrict__ in, __nv_bfloat16* __restrict__ out) {
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
     out[i] = __float2bfloat16_rn(float(in[i]));
-}
-
-// v += the element contributions in transpose-map order (deterministic mode)
-__global__ void csr_add_f32_kernel(int num_nodes, int num_elem, int elem_size, int num_comp, int64_t comp_stride,
-                                   const int* __restrict__ l_vec_indices, const int* __restrict__ t_offsets,
-                                   const int* __restrict__ t_indices, const float* __restrict__ ev,
-                                   float* __restrict__ v) {
-  for (int nd = blockIdx.x * blockDim.x + threadIdx.x; nd < num_nodes; nd += gridDim.x * blockDim.x) {
-    const int64_t l = l_vec_indices[nd];
-    const int t0 = t_offsets[nd], t1 = t_offsets[nd + 1];
-    for (int k = 0; k < num_comp; ++k) {
-      float sum = 0.0f;
-      for (int t = t0; t < t1; ++t) {
-        const int ti = t_indices[t];
-        const int e = ti / elem_size, i = ti - e * elem_size;
-        sum += ev[(int64_t(k) * elem_size + i) * num_elem + e];
-      }
-      v[l + k * comp_stride] += sum;
-    }
-  }
 }
 
 template <int P, int Q>
@@ -148,10 +129,8 @@ void lowp_apply(MassPlan& p, const S* u, float* v, cudaStream_t s) {
   if (p.evec32.size() != p.evec.size()) p.evec32.alloc(p.evec.size());
   const RestrictionData& r = *p.r;
   launch(p, qd, u, nullptr, p.evec32.get(), s);
-  csr_add_f32_kernel<<<grid_for(r.num_nodes, 256), 256, 0, s>>>(r.num_nodes, p.num_elem, p.es, p.comp_run,
-                                                                p.comp_stride, r.l_vec_indices.get(),
-                                                                r.t_offsets.get(), r.t_indices.get(),
-                                                                p.evec32.get(), v);
+  launch_csr_scatter(r.num_nodes, p.num_elem, p.es, p.comp_run, p.comp_stride, r.l_vec_indices.get(),
+                     r.t_offsets.get(), r.t_indices.get(), p.evec32.get(), v, s);
   FEM_LAUNCH_CHECK();
 }
 

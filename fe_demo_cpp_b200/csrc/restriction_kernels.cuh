@@ -11,7 +11,10 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
+
+#include "transpose_scatter.cuh"
 
 namespace fem_b200 {
 
@@ -51,30 +54,6 @@ __global__ void __launch_bounds__(kTile * 8) offset_tile_kernel(const int* __res
         atomicAdd(out + lv, __ldg(in + ev));
       else
         atomicAdd(out + lv, 1.0);
-    }
-  }
-}
-
-// Deterministic scatter-add through the transpose map: one thread per used
-// L-node, summing its E-entries in increasing t = i + e*elem_size (the order
-// of the reference's CPU scatter, src/elem-restriction.cpp:73-82, and of its
-// CUDA deterministic kernel, src/cuda/cuda-elem-restriction.cu:75-95), then
-// one add into v.
-__global__ void csr_scatter_kernel(int num_nodes, int num_elem, int elem_size, int num_comp, int64_t comp_stride,
-                                   const int* __restrict__ l_vec_indices, const int* __restrict__ t_offsets,
-                                   const int* __restrict__ t_indices, const double* __restrict__ ev,
-                                   double* __restrict__ v) {
-  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < num_nodes; n += gridDim.x * blockDim.x) {
-    const int64_t l = l_vec_indices[n];
-    const int t0 = t_offsets[n], t1 = t_offsets[n + 1];
-    for (int k = 0; k < num_comp; ++k) {
-      double sum = 0.0;
-      for (int t = t0; t < t1; ++t) {
-        const int ti = t_indices[t];
-        const int e = ti / elem_size, i = ti - e * elem_size;
-        sum += ev[(int64_t(k) * elem_size + i) * num_elem + e];
-      }
-      v[l + k * comp_stride] += sum;
     }
   }
 }

@@ -16,6 +16,7 @@
 
 #include "mass_kernels.cuh"
 #include "plan.hpp"
+#include "transpose_scatter.cuh"
 
 namespace fem_b200 {
 
@@ -248,29 +249,6 @@ __global__ void cg_update_kernel(int64_t n, const T* __restrict__ dinv, T* __res
   });
 }
 
-// v += the element contributions (deterministic mode) in transpose-map order,
-// the operator's reduction for any T; st == nullptr: outside a solve.
-template <class T>
-__global__ void csr_add_kernel(int num_nodes, int num_elem, int elem_size, int num_comp, int64_t comp_stride,
-                               const int* __restrict__ l_vec_indices, const int* __restrict__ t_offsets,
-                               const int* __restrict__ t_indices, const T* __restrict__ ev, T* __restrict__ v,
-                               const CgScalars* st) {
-  if (st && st->done) return;
-  for (int nd = blockIdx.x * blockDim.x + threadIdx.x; nd < num_nodes; nd += gridDim.x * blockDim.x) {
-    const int64_t l = l_vec_indices[nd];
-    const int t0 = t_offsets[nd], t1 = t_offsets[nd + 1];
-    for (int k = 0; k < num_comp; ++k) {
-      T sum = T(0);
-      for (int t = t0; t < t1; ++t) {
-        const int ti = t_indices[t];
-        const int e = ti / elem_size, i = ti - e * elem_size;
-        sum += ev[(int64_t(k) * elem_size + i) * num_elem + e];
-      }
-      v[l + k * comp_stride] += sum;
-    }
-  }
-}
-
 // diag[off + k*comp_stride] = diag[off] for the components k >= 1 of every
 // element node: the mass diagonal is the same for every component.
 __global__ void broadcast_comp_kernel(int64_t n, const int* __restrict__ offsets, int num_comp, int64_t comp_stride,
@@ -464,9 +442,8 @@ void assemble_diagonal(MassPlan& p, double* diag, cudaStream_t s) {
     launch(p, diag, nullptr, s);
   } else {
     launch(p, diag, p.evec.get(), s);
-    csr_add_kernel<double><<<grid_for(r.num_nodes, 256), 256, 0, s>>>(
-        r.num_nodes, p.num_elem, p.es, 1, p.comp_stride, r.l_vec_indices.get(), r.t_offsets.get(),
-        r.t_indices.get(), p.evec.get(), diag, nullptr);
+    launch_csr_scatter(r.num_nodes, p.num_elem, p.es, 1, p.comp_stride, r.l_vec_indices.get(), r.t_offsets.get(),
+                       r.t_indices.get(), p.evec.get(), diag, s);
     FEM_LAUNCH_CHECK();
   }
   if (p.comp_run > 1) {
@@ -532,10 +509,8 @@ void cg_apply(MassPlan& p, const Krylov<T>& k, cudaStream_t s) {
   }
   const RestrictionData& r = *p.r;
   k.apply(p, k.r, nullptr, k.ev, k.qd, ext, s);
-  csr_add_kernel<T><<<grid_for(r.num_nodes, 256), 256, 0, s>>>(r.num_nodes, p.num_elem, p.es, p.comp_run,
-                                                               p.comp_stride, r.l_vec_indices.get(),
-                                                               r.t_offsets.get(), r.t_indices.get(), k.ev, k.w,
-                                                               p.cg_st.get());
+  launch_csr_scatter(r.num_nodes, p.num_elem, p.es, p.comp_run, p.comp_stride, r.l_vec_indices.get(),
+                     r.t_offsets.get(), r.t_indices.get(), k.ev, k.w, s, &p.cg_st.get()->done);
   FEM_LAUNCH_CHECK();
 }
 

@@ -11,6 +11,9 @@ Two libraries, both built by ``oracle/Makefile``:
 * ``_ref/libfemref.so`` -- the reference's own src/*.cpp compiled where they
   lie, driven through its public C++ API by ref_driver.cpp.  Present wherever
   it was built (it is not in git; it travels with the working tree).
+* ``_ref/libfemrefcuda.so`` -- the reference's own CUDA restriction
+  (src/cuda/cuda-elem-restriction.cu) for sm_100a, driven by
+  ref_cuda_driver.cu: the GPU baseline of the restriction stages.
 
 ``orc`` wraps the restatement, ``ref`` the reference build; both take and
 return numpy arrays.  The restatement is pinned to the reference by
@@ -27,6 +30,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_lib", "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libfemref.so")
+REFCUDA_SO = os.path.join(HERE, "_ref", "libfemrefcuda.so")
 REF_SOURCE = "/root/reference"
 
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
@@ -40,7 +44,7 @@ def build(with_ref: bool | None = None) -> None:
     if with_ref is None:
         with_ref = os.path.isdir(os.path.join(REF_SOURCE, "src"))
     if with_ref:
-        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REF_SOURCE}"], check=True)
+        subprocess.run(["make", "-s", "-C", HERE, "ref", "refcuda", f"REF={REF_SOURCE}"], check=True)
 
 
 def _f64(a):
@@ -310,6 +314,81 @@ def ref() -> _Ref:
     if _ref is None:
         _ref = _Ref()
     return _ref
+
+
+class RefCudaRestriction:
+    """The reference's CUDA restriction (fem::cuda::elem_restriction_*) on a
+    host offsets array, with its own device L- and E-vectors; numpy in and out.
+    apply() launches on the default stream, asynchronously, as the reference."""
+
+    def __init__(self, num_elem, elem_size, num_comp, comp_stride, l_size, offsets, deterministic=False):
+        self.L = _refcuda_lib()
+        self.h = C.c_void_p()
+        self._check(self.L.refcuda_create(num_elem, elem_size, num_comp, comp_stride, l_size, _i32(offsets),
+                                          int(bool(deterministic)), C.byref(self.h)))
+        ls, es = _i64(0), _i64(0)
+        self._check(self.L.refcuda_sizes(self.h, C.byref(ls), C.byref(es)))
+        self.l_size, self.e_size = ls.value, es.value
+
+    def _check(self, rc):
+        if rc:
+            raise RuntimeError(self.L.refcuda_last_error().decode())
+
+    def set_l(self, l):
+        self._check(self.L.refcuda_set_l(self.h, _f64(l)))
+
+    def set_e(self, e):
+        self._check(self.L.refcuda_set_e(self.h, _f64(e)))
+
+    def zero_l(self):
+        self._check(self.L.refcuda_zero_l(self.h))
+
+    def apply(self, transpose):
+        self._check(self.L.refcuda_apply(self.h, int(bool(transpose))))
+
+    def get_l(self):
+        out = np.empty(self.l_size)
+        self._check(self.L.refcuda_get_l(self.h, out))
+        return out
+
+    def get_e(self):
+        out = np.empty(self.e_size)
+        self._check(self.L.refcuda_get_e(self.h, out))
+        return out
+
+    def close(self):
+        if self.h:
+            self.L.refcuda_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_refcuda = None
+
+
+def _refcuda_lib():
+    global _refcuda
+    if _refcuda is None:
+        L = C.CDLL(REFCUDA_SO)
+        L.refcuda_last_error.restype = C.c_char_p
+        L.refcuda_create.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _ip, C.c_int, C.c_void_p]
+        for name in ("refcuda_set_l", "refcuda_set_e", "refcuda_get_l", "refcuda_get_e"):
+            getattr(L, name).argtypes = [C.c_void_p, _dp]
+        for name in ("refcuda_zero_l", "refcuda_destroy"):
+            getattr(L, name).argtypes = [C.c_void_p]
+        L.refcuda_apply.argtypes = [C.c_void_p, C.c_int]
+        L.refcuda_sizes.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        _refcuda = L
+    return _refcuda
+
+
+def refcuda_available() -> bool:
+    return os.path.exists(REFCUDA_SO)
 
 
 def ref_available() -> bool:
