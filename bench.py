@@ -284,7 +284,7 @@ def run_b200(args, rank, world, local_rank):
                      "traffic": traffic, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
                      if peak_kind == "measured" else "fallback 6650 GB/s"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * N, "d2h_bytes_per_step": 8 * N,
-                "path": "fem_b200_mass_apply_host (pinned host u in, v out, synchronous)"},
+                "path": "fem_b200_mass_apply_host (pinned host u in, v out, synchronous; copies pipelined against element chunks)"},
         "clocks": clocks,
         "gpu_launches": 2 * K * launches,
     }
@@ -780,6 +780,94 @@ def run_restriction(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# end-to-end (host vectors) apply: the PCIe ceilings and the copy pipeline's
+# chunk count, on the bench workload (extra lines)
+# ---------------------------------------------------------------------------
+def run_e2e_sweep(args):
+    import torch
+    import fe_demo_cpp_b200 as fem
+    from fe_demo_cpp_b200.build import build
+    from fe_demo_cpp_b200.mesh import box_mesh
+
+    build()
+    dev = torch.device("cuda", 0)
+    mesh = box_mesh(SHAPE, P, seed=SEED)
+    N, ne = mesh.num_nodes, mesh.num_elem
+    rx = fem.Restriction(ne, P**3, 3, N, 3 * N, mesh.offsets)
+    qdata = torch.empty(Q**3 * ne, dtype=torch.float64, device=dev)
+    fem.mass_build(rx, fem.Basis(3, 3, P, Q), torch.from_numpy(mesh.coords).to(dev), qdata)
+    op = fem.MassOperator(fem.Restriction(ne, P**3, 1, N, N, mesh.offsets), fem.Basis(3, 1, P, Q), qdata)
+    del rx
+    gen = torch.Generator(device=dev).manual_seed(SEED)
+    u = torch.rand(N, dtype=torch.float64, device=dev, generator=gen) * 2 - 1
+    v = torch.empty_like(u)
+    op.autotune(u, v, reps=5)
+    u_h = u.cpu().pin_memory()
+    v_h = torch.empty(N, dtype=torch.float64).pin_memory()
+    nbytes = 8 * N
+    reps = args.e2e_steps
+
+    # the link: u in alone, v out alone, both at once (page-locked, one copy each)
+    s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
+    cur = torch.cuda.current_stream()
+
+    def copies(do_in, do_out):
+        s_in.wait_stream(cur)
+        s_out.wait_stream(cur)
+        if do_in:
+            with torch.cuda.stream(s_in):
+                u.copy_(u_h, non_blocking=True)
+        if do_out:
+            with torch.cuda.stream(s_out):
+                v_h.copy_(v, non_blocking=True)
+        cur.wait_stream(s_in)
+        cur.wait_stream(s_out)
+
+    def device_ms(fn):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    link = {"in_ms": device_ms(lambda: copies(True, False)), "out_ms": device_ms(lambda: copies(False, True)),
+            "both_ms": device_ms(lambda: copies(True, True))}
+    link.update({"in_gbs": nbytes / link["in_ms"] / 1e6, "out_gbs": nbytes / link["out_ms"] / 1e6,
+                 "both_gbs_each": nbytes / link["both_ms"] / 1e6})
+    cfg = {"mesh": "x".join(map(str, SHAPE)), "P": P, "Q": Q, "dofs": N, "bytes_each_way": nbytes}
+    print(json.dumps({"e2e": "pcie", **link, "config": cfg}), flush=True)
+
+    want = None
+    u_np, v_np = u_h.numpy(), v_h.numpy()
+    for pinned in (True, False):
+        uu, vv = (u_np, v_np) if pinned else (u_np.copy(), np.empty(N))
+        for chunks in ((1, 8, 16, 24, 32, 64) if pinned else (1, 0)):
+            op.set_host_chunks(chunks)
+            for _ in range(2):
+                op.apply_host(uu, vv)
+            ts = []
+            for _ in range(reps):
+                t0 = time.perf_counter()
+                op.apply_host(uu, vv)
+                ts.append(time.perf_counter() - t0)
+            if want is None:
+                want = vv.copy()
+            assert np.abs(vv - want).max() <= 1e-13 * np.abs(want).max()  # parity guard
+            t = statistics.median(ts)
+            print(json.dumps({"e2e": "apply_host", "host_memory": "page-locked" if pinned else "pageable",
+                              "chunks": chunks or "default", "ms": t * 1e3, "gdofs": N / t / 1e9,
+                              "vs_both_directions_at_once": link["both_ms"] / (t * 1e3), "config": cfg}),
+                  flush=True)
+    op.set_host_chunks(0)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -811,7 +899,12 @@ def main():
     ap.add_argument("--restriction", action="store_true",
                     help="restriction stages vs the reference's CUDA kernels (extra lines)")
     ap.add_argument("--restriction-steps", type=int, default=20)
+    ap.add_argument("--e2e-sweep", action="store_true",
+                    help="host-vector apply: PCIe ceilings and copy-pipeline chunk counts (extra lines)")
+    ap.add_argument("--e2e-steps", type=int, default=10)
     args = ap.parse_args()
+    if args.e2e_sweep:
+        return run_e2e_sweep(args)
     if args.restriction:
         return run_restriction(args)
     if args.serve:

@@ -288,6 +288,10 @@ class MassOperator(_Handle):
     def set_kernel(self, variant) -> None:
         call("fem_b200_mass_set_kernel", self.h, int(variant))
 
+    def set_host_chunks(self, chunks: int) -> None:
+        """Chunks of apply_host's copy pipeline: 0 default, 1 unpipelined, n about n."""
+        call("fem_b200_mass_set_host_chunks", self.h, int(chunks))
+
     def autotune(self, u, v, reps: int = 10, stream=None):
         """Time every kernel variant on (u, v) (v is scratch), keep the fastest;
         returns (variant name, ms per apply)."""

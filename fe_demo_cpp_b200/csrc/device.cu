@@ -45,8 +45,8 @@ void launch_apply3(const MassPlan& p, const double* u, double* v, double* ev, cu
   using L = Mass3D<P, Q>;
   static std::atomic<uint64_t> smem_set{0};
   set_smem(mass3d_apply_kernel<P, Q, MINB>, L::SMEM, smem_set);
-  mass3d_apply_kernel<P, Q, MINB><<<unsigned(p.n_tiles), L::NT, L::SMEM, s>>>(
-      make_mat<P, Q>(p.basis), p.offs_t.get(), p.qd_t.get(), u, v, ev, p.num_elem, p.comp_run, p.comp_stride,
+  mass3d_apply_kernel<P, Q, MINB><<<unsigned(p.tiles()), L::NT, L::SMEM, s>>>(
+      make_mat<P, Q>(p.basis), p.offs(), p.qd(), u, v, ev, p.elems(), p.comp_run, p.comp_stride,
       ApplyPlain{});
   FEM_LAUNCH_CHECK();
 }
@@ -63,10 +63,10 @@ void launch_apply3_pipe(const MassPlan& p, const double* u, double* v, double* e
   using L = Pipe3D<P, Q>;
   static std::atomic<uint64_t> smem_set{0};
   set_smem(mass3d_apply_pipe_kernel<P, Q>, L::SMEM, smem_set);
-  const int grid = persistent_grid(mass3d_apply_pipe_kernel<P, Q>, L::NT, L::SMEM, p.n_tiles);
-  mass3d_apply_pipe_kernel<P, Q><<<grid, L::NT, L::SMEM, s>>>(make_mat<P, Q>(p.basis), p.offs_t.get(),
-                                                               p.qd_t.get(), u, v, ev, p.num_elem, p.comp_run,
-                                                               p.comp_stride, p.n_tiles, p.status.get());
+  const int grid = persistent_grid(mass3d_apply_pipe_kernel<P, Q>, L::NT, L::SMEM, p.tiles());
+  mass3d_apply_pipe_kernel<P, Q><<<grid, L::NT, L::SMEM, s>>>(make_mat<P, Q>(p.basis), p.offs(),
+                                                               p.qd(), u, v, ev, p.elems(), p.comp_run,
+                                                               p.comp_stride, p.tiles(), p.status.get());
   FEM_LAUNCH_CHECK();
 }
 
@@ -76,10 +76,10 @@ void launch_apply3_pf(const MassPlan& p, const double* u, double* v, double* ev,
   constexpr int smem = Prefetch3D<P, Q>::SMEM;
   static std::atomic<uint64_t> smem_set{0};
   set_smem(mass3d_apply_prefetch_kernel<P, Q>, smem, smem_set);
-  const int grid = persistent_grid(mass3d_apply_prefetch_kernel<P, Q>, L::NT, smem, p.n_tiles);
-  mass3d_apply_prefetch_kernel<P, Q><<<grid, L::NT, smem, s>>>(make_mat<P, Q>(p.basis), p.offs_t.get(),
-                                                                p.qd_t.get(), u, v, ev, p.num_elem, p.comp_run,
-                                                                p.comp_stride, int(p.n_tiles), p.status.get());
+  const int grid = persistent_grid(mass3d_apply_prefetch_kernel<P, Q>, L::NT, smem, p.tiles());
+  mass3d_apply_prefetch_kernel<P, Q><<<grid, L::NT, smem, s>>>(make_mat<P, Q>(p.basis), p.offs(),
+                                                                p.qd(), u, v, ev, p.elems(), p.comp_run,
+                                                                p.comp_stride, int(p.tiles()), p.status.get());
   FEM_LAUNCH_CHECK();
 }
 
@@ -88,9 +88,9 @@ void launch_apply3_x2(const MassPlan& p, const double* u, double* v, double* ev,
   using L = Mass3DX2<P, Q>;
   static std::atomic<uint64_t> smem_set{0};
   set_smem(mass3d_apply_x2_kernel<P, Q>, L::SMEM, smem_set);
-  const unsigned grid = unsigned((p.n_tiles + 1) / 2);  // the plan's tile arrays hold an even number of tiles
-  mass3d_apply_x2_kernel<P, Q><<<grid, L::NT, L::SMEM, s>>>(make_mat<P, Q>(p.basis), p.offs_t.get(), p.qd_t.get(),
-                                                             u, v, ev, p.num_elem, p.comp_run, p.comp_stride);
+  const unsigned grid = unsigned((p.tiles() + 1) / 2);  // the plan's tile arrays hold an even number of tiles
+  mass3d_apply_x2_kernel<P, Q><<<grid, L::NT, L::SMEM, s>>>(make_mat<P, Q>(p.basis), p.offs(), p.qd(),
+                                                             u, v, ev, p.elems(), p.comp_run, p.comp_stride);
   FEM_LAUNCH_CHECK();
 }
 
@@ -104,17 +104,17 @@ void launch_apply3_narrow(const MassPlan& p, const double* u, double* v, double*
   const auto kern = mass3d_apply_narrow_kernel<P, Q, minb>;
   static std::atomic<uint64_t> smem_set{0};
   set_smem(kern, L::SMEM, smem_set);
-  kern<<<unsigned(2 * p.n_tiles), L::NT, L::SMEM, s>>>(make_mat<P, Q>(p.basis), p.offs_t.get(), p.qd_t.get(), u,
-                                                       v, ev, p.num_elem, p.comp_run, p.comp_stride);
+  kern<<<unsigned(2 * p.tiles()), L::NT, L::SMEM, s>>>(make_mat<P, Q>(p.basis), p.offs(), p.qd(), u,
+                                                       v, ev, p.elems(), p.comp_run, p.comp_stride);
   FEM_LAUNCH_CHECK();
 }
 
 // One element per thread (P <= 3): 128-thread CTAs over the plan's elements.
 template <int P, int Q>
 void launch_apply3_element(const MassPlan& p, const double* u, double* v, double* ev, cudaStream_t s) {
-  const unsigned grid = unsigned((p.n_tiles * 8 + 127) / 128);
-  mass3d_apply_element_kernel<P, Q><<<grid, 128, 0, s>>>(make_mat<P, Q>(p.basis), p.offs_t.get(), p.qd_t.get(), u,
-                                                          v, ev, p.num_elem, p.comp_run, p.comp_stride);
+  const unsigned grid = unsigned((p.tiles() * 8 + 127) / 128);
+  mass3d_apply_element_kernel<P, Q><<<grid, 128, 0, s>>>(make_mat<P, Q>(p.basis), p.offs(), p.qd(), u,
+                                                          v, ev, p.elems(), p.comp_run, p.comp_stride);
   FEM_LAUNCH_CHECK();
 }
 
@@ -123,16 +123,16 @@ void launch_apply2(const MassPlan& p, const double* u, double* v, double* ev, cu
   using L = Mass2D<P, Q>;
   static std::atomic<uint64_t> smem_set{0};
   set_smem(mass2d_apply_kernel<P, Q>, L::SMEM, smem_set);
-  mass2d_apply_kernel<P, Q><<<unsigned(p.n_tiles), L::NT, L::SMEM, s>>>(
-      make_mat<P, Q>(p.basis), p.offs_t.get(), p.qd_t.get(), u, v, ev, p.num_elem, p.comp_run, p.comp_stride,
+  mass2d_apply_kernel<P, Q><<<unsigned(p.tiles()), L::NT, L::SMEM, s>>>(
+      make_mat<P, Q>(p.basis), p.offs(), p.qd(), u, v, ev, p.elems(), p.comp_run, p.comp_stride,
       ApplyPlain{});
   FEM_LAUNCH_CHECK();
 }
 
 template <int P, int Q>
 void launch_apply1(const MassPlan& p, const double* u, double* v, double* ev, cudaStream_t s) {
-  mass1d_apply_kernel<P, Q><<<unsigned(p.n_tiles), 128, 0, s>>>(make_mat<P, Q>(p.basis), p.offs_t.get(),
-                                                                 p.qd_t.get(), u, v, ev, p.num_elem, p.comp_run,
+  mass1d_apply_kernel<P, Q><<<unsigned(p.tiles()), 128, 0, s>>>(make_mat<P, Q>(p.basis), p.offs(),
+                                                                 p.qd(), u, v, ev, p.elems(), p.comp_run,
                                                                  p.comp_stride, ApplyPlain{});
   FEM_LAUNCH_CHECK();
 }
@@ -1005,12 +1005,24 @@ int fem_b200_mass_apply_host(fem_b200_mass op, const double* u_host, int64_t n_u
     cudaStream_t s = as_stream(stream);
     if (p.hu.size() != size_t(p.l_size)) p.hu.alloc(size_t(p.l_size));
     if (p.hv.size() != size_t(p.l_size)) p.hv.alloc(size_t(p.l_size));
-    const size_t bytes = size_t(p.l_size) * sizeof(double);
-    FEM_CUDA_CHECK(cudaMemcpyAsync(p.hu.get(), u_host, bytes, cudaMemcpyHostToDevice, s));
-    mass_apply_impl(p, p.hu.get(), p.hv.get(), true, s);
-    FEM_CUDA_CHECK(cudaMemcpyAsync(v_host, p.hv.get(), bytes, cudaMemcpyDeviceToHost, s));
-    FEM_CUDA_CHECK(cudaStreamSynchronize(s));
+    if (host_pipeline_applies(p)) {
+      mass_apply_host_pipelined(p, u_host, v_host, s);
+    } else {
+      const size_t bytes = size_t(p.l_size) * sizeof(double);
+      FEM_CUDA_CHECK(cudaMemcpyAsync(p.hu.get(), u_host, bytes, cudaMemcpyHostToDevice, s));
+      mass_apply_impl(p, p.hu.get(), p.hv.get(), true, s);
+      FEM_CUDA_CHECK(cudaMemcpyAsync(v_host, p.hv.get(), bytes, cudaMemcpyDeviceToHost, s));
+      FEM_CUDA_CHECK(cudaStreamSynchronize(s));
+    }
     check_status(p);
+  });
+}
+
+int fem_b200_mass_set_host_chunks(fem_b200_mass op, int chunks) {
+  return guarded([&] {
+    require(op && op->d, "mass_set_host_chunks: NULL handle");
+    require(chunks >= 0 && chunks <= 4096, "mass_set_host_chunks: chunks must be in 0..4096");
+    op->d->host_chunks = chunks;
   });
 }
 

@@ -175,6 +175,25 @@ struct BasisDev {
 // ---------------------------------------------------------------------------
 // Mass plan
 // ---------------------------------------------------------------------------
+// The host-memory apply's pipeline state (host_apply.cu): copy streams,
+// events and the element chunks with the L-vector node span each touches.
+struct HostPipeline {
+  cudaStream_t h2d = nullptr, d2h = nullptr;
+  std::vector<cudaEvent_t> ev;  // 2 + 2 per chunk: start, v zeroed, then (u span in, chunk applied)
+  int64_t tiles_per_chunk = 0;
+  int target = 0;               // the chunk count it was built for
+  std::vector<int64_t> lo, hi;  // per chunk: smallest and largest offset of its elements
+  HostPipeline() = default;
+  HostPipeline(const HostPipeline&) = delete;
+  HostPipeline& operator=(const HostPipeline&) = delete;
+  ~HostPipeline() {
+    for (cudaEvent_t e : ev)
+      if (e) (void)cudaEventDestroy(e);
+    if (h2d) (void)cudaStreamDestroy(h2d);
+    if (d2h) (void)cudaStreamDestroy(d2h);
+  }
+};
+
 struct MassPlan;
 using ApplyLauncher = void (*)(const MassPlan&, const double*, double*, double*, cudaStream_t);
 using BuildLauncher = void (*)(const BasisData&, const RestrictionData&, const double*, double*, cudaStream_t);
@@ -192,6 +211,18 @@ struct MassPlan {
   DevBuf<double> qd_t;
   DevBuf<double> evec;    // deterministic mode: element contributions
   DevBuf<double> hu, hv;  // staging for the host-memory apply
+  std::unique_ptr<HostPipeline> pipe;
+  int host_chunks = 0;  // host-memory apply: 0 default, 1 unpipelined, n >= 2 about n chunks
+  // The tile range the apply launchers cover: every tile, or span_tiles
+  // tiles from span_first (an element chunk of the host-memory apply; atomic
+  // scatter only, where the element index serves only the bounds check).
+  int64_t span_first = 0, span_tiles = -1;
+  const int* offs() const { return offs_t.get() + span_first * es * tile_e; }
+  const double* qd() const { return qd_t.get() + span_first * int64_t(nq) * tile_e; }
+  int64_t tiles() const { return span_tiles < 0 ? n_tiles : span_tiles; }
+  int elems() const {
+    return span_tiles < 0 ? num_elem : int(std::min<int64_t>(span_tiles * tile_e, num_elem - span_first * tile_e));
+  }
   DevBuf<int> status;     // device status word (bit 0: a bounded wait ran out)
   ApplyLauncher launch = nullptr;       // the kernel in use
   ApplyLauncher launch_simple = nullptr;
@@ -267,6 +298,12 @@ void set_smem(K kernel, int bytes, std::atomic<uint64_t>& done) {
 // Defined in device.cu.
 void check_status(MassPlan& p, cudaStream_t s = nullptr);
 void mass_apply_impl(MassPlan& p, const double* u, double* v, bool zero, cudaStream_t s);
+// The host-memory apply with its copies pipelined against the element chunks
+// (host_apply.cu); host_pipeline_applies says whether the plan qualifies
+// (atomic scatter, at least two chunks, not set to unpipelined).
+// Synchronous: returns with v_host written.
+bool host_pipeline_applies(const MassPlan& p);
+void mass_apply_host_pipelined(MassPlan& p, const double* u_host, double* v_host, cudaStream_t s);
 std::string shape_str(int dim, int P, int Q);
 // A fused apply and build kernel exist for (dim, P, Q).
 bool device_path_supported(int dim, int P, int Q);

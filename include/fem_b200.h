@@ -279,10 +279,22 @@ int fem_b200_mass_apply(fem_b200_mass op, const double *u, int64_t n_u, double *
 int fem_b200_mass_apply_add(fem_b200_mass op, const double *u, int64_t n_u, double *v, int64_t n_v, void *stream);
 
 /* Host-memory form of fem_b200_mass_apply: copies u in, applies, copies v out
- * on `stream` through plan-owned device buffers, then synchronizes the stream.
- * The call a host std::vector user makes (operator_apply(op, in, out)). */
+ * through plan-owned device buffers, and returns with v_host written.  The
+ * call a host std::vector user makes (operator_apply(op, in, out)).  With the
+ * atomic scatter and at least 1024 tiles of elements the copies are
+ * pipelined: u comes in by node span on a plan-owned stream, the kernels run
+ * per element chunk on `stream` as their span arrives, and v goes out on a
+ * second plan-owned stream as each range becomes final, so the two PCIe
+ * directions overlap (page-locked or pageable host memory; the plan is not
+ * to be used from two threads at once).  Otherwise: copy in, apply, copy out
+ * on `stream`. */
 int fem_b200_mass_apply_host(fem_b200_mass op, const double *u_host, int64_t n_u, double *v_host, int64_t n_v,
                              void *stream);
+
+/* Chunks of the host-memory apply's pipeline: 0 the default (about 24), 1 no
+ * pipelining (copy in, apply, copy out), n >= 2 about n chunks (each at least
+ * 512 tiles).  Takes effect at the next fem_b200_mass_apply_host. */
+int fem_b200_mass_set_host_chunks(fem_b200_mass op, int chunks);
 
 /* Number of kernel launches one fem_b200_mass_apply makes, the plan's
  * element-tile size, device footprint in bytes and the kernel variant in use
