@@ -16,6 +16,14 @@
 // degenerates to copy-in, apply, copy-out.  Only the atomic scatter is
 // pipelined (the deterministic one reduces over all elements at the end).
 //
+// Pageable host vectors: the DMA engines reach pageable memory only through
+// the driver's own staging (about 13 GB/s a direction), and page-locking the
+// caller's vectors per call costs more than the copy (42 ms to register a
+// touched 0.5 GB).  So each pageable direction goes through a plan-owned
+// ring of page-locked slots, filled or drained by a pool of host memcpy
+// threads while the DMA engines move the other slots: u by this thread ahead
+// of each chunk, v by a second thread behind each chunk.
+//
 // Components: with the blocked layout (comp_stride past the node span) each
 // component's window is pipelined on its own; otherwise one window covers
 // [lo, hi + (components - 1) * comp_stride].  L entries outside every window
@@ -111,6 +119,22 @@ bool page_locked(const void* ptr) {
   return a.type == cudaMemoryTypeHost;
 }
 
+// Staging of pageable host vectors: a page-locked ring of kSlots slots of
+// kSlotElems doubles (8 MB) per direction.  A slot is filled (or drained) by
+// the memcpy pool while the DMA engines move the others.
+constexpr int kSlots = 6;
+constexpr int64_t kSlotElems = int64_t(1) << 20;
+
+void ensure_staging(HostPipeline& hp) {
+  if (hp.pool) return;
+  hp.ring_in.alloc(size_t(kSlots * kSlotElems));
+  hp.ring_out.alloc(size_t(kSlots * kSlotElems));
+  hp.slot_ev.assign(size_t(2 * kSlots), nullptr);
+  for (cudaEvent_t& e : hp.slot_ev) FEM_CUDA_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  const unsigned hw = std::thread::hardware_concurrency();
+  hp.pool = std::make_unique<CopyPool>(int(std::min(8u, std::max(2u, hw / 2))));
+}
+
 struct Copy {
   int chunk;  // -1: after v is zeroed, else after this chunk's apply
   int64_t first, count;
@@ -196,21 +220,31 @@ void mass_apply_host_pipelined(MassPlan& p, const double* u_host, double* v_host
       }
   }
 
-  // a page-locked v is copied out from this thread; into pageable memory each
-  // copy blocks its caller until it is done, so a second thread issues them,
-  // each once this thread has recorded the event it waits on (a wait on an
-  // event not yet recorded would not wait)
-  const bool v_locked = page_locked(v_host);
-  auto issue_out = [&](const Copy& o) {
-    FEM_CUDA_CHECK(cudaStreamWaitEvent(hp.d2h, o.chunk < 0 ? ev_zero : hp.ev[size_t(3 + 2 * o.chunk)], 0));
-    FEM_CUDA_CHECK(cudaMemcpyAsync(v_host + o.first, hv + o.first, size_t(o.count) * sizeof(double),
-                                   cudaMemcpyDeviceToHost, hp.d2h));
-  };
+  // Page-locked v: the copies out are issued from this thread, each after its
+  // chunk's apply.  Pageable v: a second thread drains them through the
+  // staging ring, each copy issued once this thread has recorded the event it
+  // waits on (a wait on an event not yet recorded would not wait).
+  // Pageable u: this thread fills the input ring ahead of each chunk.
+  const bool u_locked = page_locked(u_host), v_locked = page_locked(v_host);
+  if (!u_locked || !v_locked) ensure_staging(hp);
+  if (!v_locked) {  // ring-sized pieces
+    std::vector<Copy> split;
+    for (const Copy& o : out)
+      for (int64_t off = 0; off < o.count; off += kSlotElems)
+        split.push_back({o.chunk, o.first + off, std::min(kSlotElems, o.count - off)});
+    out.swap(split);
+  }
+  auto chunk_event = [&](int chunk) { return chunk < 0 ? ev_zero : hp.ev[size_t(3 + 2 * chunk)]; };
   size_t next_out = 0;
   Writer w;
   auto publish = [&](int c) {
     if (v_locked) {
-      for (; next_out < out.size() && out[next_out].chunk <= c; ++next_out) issue_out(out[next_out]);
+      for (; next_out < out.size() && out[next_out].chunk <= c; ++next_out) {
+        const Copy& o = out[next_out];
+        FEM_CUDA_CHECK(cudaStreamWaitEvent(hp.d2h, chunk_event(o.chunk), 0));
+        FEM_CUDA_CHECK(cudaMemcpyAsync(v_host + o.first, hv + o.first, size_t(o.count) * sizeof(double),
+                                       cudaMemcpyDeviceToHost, hp.d2h));
+      }
     } else {
       {
         std::lock_guard<std::mutex> lock(w.mu);
@@ -224,13 +258,32 @@ void mass_apply_host_pipelined(MassPlan& p, const double* u_host, double* v_host
     w.th = std::thread([&, dev] {
       try {
         FEM_CUDA_CHECK(cudaSetDevice(dev));
-        for (const Copy& o : out) {
-          {
-            std::unique_lock<std::mutex> lock(w.mu);
-            w.cv.wait(lock, [&] { return w.abort || w.recorded >= o.chunk; });
-            if (w.recorded < o.chunk) return;  // aborted
+        auto recorded = [&](int chunk, bool block) {  // false: not yet (block = false) or aborted
+          std::unique_lock<std::mutex> lock(w.mu);
+          if (block) w.cv.wait(lock, [&] { return w.abort || w.recorded >= chunk; });
+          return w.recorded >= chunk;
+        };
+        auto issue = [&](size_t k) {
+          const Copy& o = out[k];
+          double* slot = hp.ring_out.get() + int64_t(k % kSlots) * kSlotElems;
+          FEM_CUDA_CHECK(cudaStreamWaitEvent(hp.d2h, chunk_event(o.chunk), 0));
+          FEM_CUDA_CHECK(cudaMemcpyAsync(slot, hv + o.first, size_t(o.count) * sizeof(double),
+                                         cudaMemcpyDeviceToHost, hp.d2h));
+          FEM_CUDA_CHECK(cudaEventRecord(hp.slot_ev[size_t(kSlots) + k % kSlots], hp.d2h));
+        };
+        size_t issued = 0;
+        for (size_t j = 0; j < out.size(); ++j) {
+          for (; issued <= j; ++issued) {
+            if (!recorded(out[issued].chunk, true)) return;  // aborted
+            issue(issued);
           }
-          issue_out(o);
+          // keep the ring's other slots in flight: piece k reuses the slot of
+          // piece k - kSlots, whose copy to v_host is done (k < j + kSlots)
+          for (; issued < out.size() && issued < j + kSlots && recorded(out[issued].chunk, false); ++issued)
+            issue(issued);
+          FEM_CUDA_CHECK(cudaEventSynchronize(hp.slot_ev[size_t(kSlots) + j % kSlots]));
+          hp.pool->copy(v_host + out[j].first, hp.ring_out.get() + int64_t(j % kSlots) * kSlotElems,
+                        size_t(out[j].count) * sizeof(double));
         }
       } catch (const std::exception& e) {
         w.error = e.what();
@@ -239,15 +292,33 @@ void mass_apply_host_pipelined(MassPlan& p, const double* u_host, double* v_host
   }
   publish(-1);
 
+  int64_t k_in = 0;  // ring pieces copied in so far (pageable u)
+  auto copy_in = [&](int64_t first, int64_t count) {
+    if (u_locked) {
+      FEM_CUDA_CHECK(cudaMemcpyAsync(hu + first, u_host + first, size_t(count) * sizeof(double),
+                                     cudaMemcpyHostToDevice, hp.h2d));
+      return;
+    }
+    for (int64_t off = 0; off < count; off += kSlotElems, ++k_in) {
+      const int64_t n = std::min(kSlotElems, count - off);
+      const int slot = int(k_in % kSlots);
+      cudaEvent_t e = hp.slot_ev[size_t(slot)];
+      FEM_CUDA_CHECK(cudaEventSynchronize(e));  // the slot's previous copy is done (never recorded: at once)
+      double* st = hp.ring_in.get() + int64_t(slot) * kSlotElems;
+      hp.pool->copy(st, u_host + first + off, size_t(n) * sizeof(double));
+      FEM_CUDA_CHECK(cudaMemcpyAsync(hu + first + off, st, size_t(n) * sizeof(double), cudaMemcpyHostToDevice,
+                                     hp.h2d));
+      FEM_CUDA_CHECK(cudaEventRecord(e, hp.h2d));
+    }
+  };
+
   SpanReset reset{p};
   std::vector<int64_t> in_done(size_t(n_win), w_lo);
   for (int c = 0; c < n_chunks; ++c) {
     for (int k = 0; k < n_win; ++k) {
       const int64_t end = hp.hi[c] + ext + 1;
       if (end > in_done[k]) {
-        const int64_t first = in_done[k] + k * w_step;
-        FEM_CUDA_CHECK(cudaMemcpyAsync(hu + first, u_host + first, size_t(end - in_done[k]) * sizeof(double),
-                                       cudaMemcpyHostToDevice, hp.h2d));
+        copy_in(in_done[k] + k * w_step, end - in_done[k]);
         in_done[k] = end;
       }
     }

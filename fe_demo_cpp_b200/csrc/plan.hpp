@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "common.hpp"
+#include "copy_pool.hpp"
 #include "fem_b200.h"
 #include "host_setup.hpp"
 #include "mass_kernels.cuh"
@@ -183,10 +184,18 @@ struct HostPipeline {
   int64_t tiles_per_chunk = 0;
   int target = 0;               // the chunk count it was built for
   std::vector<int64_t> lo, hi;  // per chunk: smallest and largest offset of its elements
+  // staging for pageable host vectors, made by the first such apply: a ring
+  // of page-locked slots per direction, an event per slot, a memcpy pool
+  PinnedBuf<double> ring_in, ring_out;
+  std::vector<cudaEvent_t> slot_ev;  // kSlots for the copies in, then kSlots for the copies out
+  std::unique_ptr<CopyPool> pool;
   HostPipeline() = default;
   HostPipeline(const HostPipeline&) = delete;
   HostPipeline& operator=(const HostPipeline&) = delete;
   ~HostPipeline() {
+    pool.reset();
+    for (cudaEvent_t e : slot_ev)
+      if (e) (void)cudaEventDestroy(e);
     for (cudaEvent_t e : ev)
       if (e) (void)cudaEventDestroy(e);
     if (h2d) (void)cudaStreamDestroy(h2d);

@@ -9,7 +9,9 @@ becomes final.  Each case compares it with the device apply of the same plan
 case with the oracle.  Cases: page-locked and pageable host buffers, every
 3D kernel variant, blocked and interleaved vector fields, the reference's
 component-0-only apply_mass on a 3-component field, node numberings that
-defeat the pipeline (scrambled, elements in reverse), 2D, the chunk setting.
+defeat the pipeline (scrambled, elements in reverse), 2D, the chunk setting,
+mixed page-locked / pageable pairs, and a mesh large enough that the
+pageable staging ring wraps and splits copies across slots.
 """
 import numpy as np
 import pytest
@@ -38,21 +40,21 @@ def _qdata(fem, cuda, m, Q):
     return qd
 
 
-def _both(fem, cuda, op, l_size, seed, pinned):
-    """(host apply, device apply) of the same u."""
+def _both(fem, cuda, op, l_size, seed, pinned, pinned_v=None):
+    """(host apply, device apply) of the same u; `pinned` / `pinned_v`: the
+    host u / v page-locked (v like u unless given), else pageable."""
     import torch
+    pinned_v = pinned if pinned_v is None else pinned_v
     u = random_vector(l_size, seed)
     v_dev = torch.empty(l_size, dtype=torch.float64, device=cuda)
     op.apply(torch.from_numpy(u).to(cuda), v_dev)
     torch.cuda.synchronize()
-    if pinned:
-        u_h = torch.from_numpy(u).pin_memory()
-        v_h = torch.full((l_size,), np.nan, dtype=torch.float64).pin_memory()
-        op.apply_host(u_h.numpy(), v_h.numpy())
-        got = v_h.numpy().copy()
-    else:
-        got = op.apply_host(u, np.full(l_size, np.nan))
-    return got, v_dev.cpu().numpy()
+    u_h = torch.from_numpy(u).pin_memory() if pinned else torch.from_numpy(u.copy())
+    v_h = torch.full((l_size,), np.nan, dtype=torch.float64)
+    if pinned_v:
+        v_h = v_h.pin_memory()
+    op.apply_host(u_h.numpy(), v_h.numpy())
+    return v_h.numpy().copy(), v_dev.cpu().numpy()
 
 
 @pytest.fixture(scope="module")
@@ -145,3 +147,26 @@ def test_host_chunk_setting(fem, cuda, mesh3):
         close(got, want)
     with pytest.raises(Exception):
         op.set_host_chunks(-1)
+
+
+@pytest.mark.parametrize("pinned_u,pinned_v", [(True, False), (False, True)], ids=["u-locked", "v-locked"])
+def test_pipelined_host_apply_mixed_memory(fem, cuda, mesh3, pinned_u, pinned_v):
+    m, qd = mesh3
+    op = _scalar_op(fem, m, qd)
+    got, want = _both(fem, cuda, op, m.num_nodes, 21, pinned_u, pinned_v)
+    close(got, want)
+
+
+def test_pageable_staging_ring_wraps(fem, cuda):
+    """140^3 hexes at P = 2 (2.8M nodes, 343,000 tiles): 24 chunks give dozens
+    of ring pieces a direction (the 6-slot ring wraps); 2 chunks give copies of
+    1.4M nodes, split over slots of 1M doubles."""
+    m = box_mesh((140, 140, 140), 2, seed=7)
+    qd = _qdata(fem, cuda, m, 3)
+    op = fem.MassOperator(fem.Restriction(m.num_elem, 8, 1, m.num_nodes, m.num_nodes, m.offsets),
+                          fem.Basis(3, 1, 2, 3), qd)
+    for chunks in (0, 2):
+        op.set_host_chunks(chunks)
+        for rep in range(2):  # the second call reuses the ring and its events
+            got, want = _both(fem, cuda, op, m.num_nodes, 30 + rep, False)
+            close(got, want)
