@@ -246,8 +246,22 @@ ApplyLauncher variant_launcher(const MassPlan& p, int variant) {
   }
 }
 
+// The variant a plan runs until it is autotuned: where one variant beat the
+// one-tile kernel on every B200 of the order sweep (64M-DoF box meshes,
+// Q = P + 1, one and three components), that one; else the one-tile kernel.
+// element at P <= 3 (P = 2: 2.5x, P = 3: 1.1-1.15x), prefetch at P = 7
+// (1.2-1.35x), narrow at P = 8 (1.5x).  Other orders and quadratures: their
+// best variant moves from box to box, which the autotuner settles.
+int default_variant(const MassPlan& p) {
+  if (p.dim != 3 || p.Q != p.P + 1) return FEM_B200_KERNEL_SIMPLE;
+  if (p.P <= 3) return FEM_B200_KERNEL_ELEMENT;
+  if (p.P == 7) return FEM_B200_KERNEL_PREFETCH;
+  if (p.P == 8) return FEM_B200_KERNEL_NARROW;
+  return FEM_B200_KERNEL_SIMPLE;
+}
+
 // The variant FEM_B200_KERNEL_AUTO selects for a plan: the autotuned choice
-// for its key if there is one, else the one-tile kernel.
+// for its key if there is one, else default_variant.
 ApplyLauncher auto_kernel(const MassPlan& p) {
   std::lock_guard<std::mutex> lock(g_tune_mu);
   auto it = g_tune.find(tune_key(p));
@@ -255,7 +269,8 @@ ApplyLauncher auto_kernel(const MassPlan& p) {
     ApplyLauncher l = variant_launcher(p, it->second);
     if (l) return l;
   }
-  return p.launch_simple;
+  ApplyLauncher l = variant_launcher(p, default_variant(p));
+  return l ? l : p.launch_simple;
 }
 
 bool fused_supported(int dim, int P, int Q) {
