@@ -44,8 +44,10 @@ def algorithmic_bytes(num_elem, num_nodes, P, Q, nc=1, dim=3):
     return num_elem * (4 * P**dim + 8 * Q**dim) + 16 * nc * num_nodes
 
 
-def algorithmic_flops(num_elem, P, Q, nc=1):
-    """Sum-factorised flops of one apply (3D): interp + interp^T + pointwise."""
+def algorithmic_flops(num_elem, P, Q, nc=1, dim=3):
+    """Sum-factorised flops of one apply: interp + interp^T + pointwise."""
+    if dim == 2:
+        return num_elem * nc * (4 * (P**2 * Q + P * Q**2) + Q**2)
     return num_elem * nc * (4 * (P**3 * Q + P**2 * Q**2 + P * Q**3) + Q**3)
 
 
@@ -313,25 +315,25 @@ def run_sweep(args):
     dev = torch.device("cuda", 0)
     peak, _ = measured_peaks()
     Ps = [int(p) for p in args.sweep_P.split(",")]
-    for Pp in Ps:
+    for dim, Pp in [(d, p) for d in (int(x) for x in args.sweep_dim.split(",")) for p in Ps]:
         Qq = Pp + 1
         for nc in (1, 3):
-            shape = mesh_for_dofs(64_000_000 // nc, Pp)
+            shape = mesh_for_dofs(64_000_000 // nc, Pp, dim)
             m = box_mesh_device(shape, Pp, seed=SEED, device=dev)
             N, ne = m.num_nodes, m.num_elem
             offs = m.offsets.cpu().numpy()
-            rx = fem.Restriction(ne, Pp**3, 3, N, 3 * N, offs)
-            bx = fem.Basis(3, 3, Pp, Qq)
-            qd = torch.empty(Qq**3 * ne, dtype=torch.float64, device=dev)
+            rx = fem.Restriction(ne, Pp**dim, dim, N, dim * N, offs)
+            bx = fem.Basis(dim, dim, Pp, Qq)
+            qd = torch.empty(Qq**dim * ne, dtype=torch.float64, device=dev)
             fem.mass_build(rx, bx, m.coords, qd)
             del rx, bx
             m.coords = None
-            ru = fem.Restriction(ne, Pp**3, nc, N, nc * N, offs)
-            bu = fem.Basis(3, nc, Pp, Qq)
+            ru = fem.Restriction(ne, Pp**dim, nc, N, nc * N, offs)
+            bu = fem.Basis(dim, nc, Pp, Qq)
             op = fem.MassOperator(ru, bu, qd, fem.QF.apply_mass_vector if nc > 1 else fem.QF.apply_mass)
             u = torch.rand(nc * N, dtype=torch.float64, device=dev) * 2 - 1
             v = torch.empty_like(u)
-            abytes = algorithmic_bytes(ne, N, Pp, Qq, nc)
+            abytes = algorithmic_bytes(ne, N, Pp, Qq, nc, dim)
             for variant in fem.KernelVariant:
                 if variant == fem.KernelVariant.auto:
                     continue
@@ -349,18 +351,19 @@ def run_sweep(args):
                 t1.record()
                 torch.cuda.synchronize()
                 kms = t0.elapsed_time(t1) / args.sweep_steps
-                print(json.dumps({"sweep": "mass_apply", "P": Pp, "Q": Qq, "num_comp": nc, "mesh": list(shape),
+                print(json.dumps({"sweep": "mass_apply", "dim": dim, "P": Pp, "Q": Qq, "num_comp": nc,
+                                  "mesh": list(shape),
                                   "dofs": nc * N, "kernel": variant.name, "kernel_ms": kms,
                                   "gdofs_kernel": nc * N / kms / 1e6,
                                   "roofline_frac": abytes / (kms * 1e-3) / 1e9 / peak,
-                                  "fp64_tflops": algorithmic_flops(ne, Pp, Qq, nc) / (kms * 1e-3) / 1e12}),
+                                  "fp64_tflops": algorithmic_flops(ne, Pp, Qq, nc, dim) / (kms * 1e-3) / 1e12}),
                       flush=True)
             # reduced storage: FP32 (u, v, qdata) and BF16 (u, qdata; FP32 v), public applies
             for name, uu, vv, ab in (
                     ("fp32", u.float(), torch.empty(nc * N, dtype=torch.float32, device=dev),
-                     ne * (4 * Pp**3 + 4 * Qq**3) + 8 * nc * N),
+                     ne * (4 * Pp**dim + 4 * Qq**dim) + 8 * nc * N),
                     ("bf16", u.to(torch.bfloat16), torch.empty(nc * N, dtype=torch.float32, device=dev),
-                     ne * (4 * Pp**3 + 2 * Qq**3) + 6 * nc * N)):
+                     ne * (4 * Pp**dim + 2 * Qq**dim) + 6 * nc * N)):
                 fn = op.apply_f32 if name == "fp32" else op.apply_bf16
                 for _ in range(3):
                     fn(uu, vv)
@@ -371,7 +374,8 @@ def run_sweep(args):
                 e1.record()
                 torch.cuda.synchronize()
                 ms = e0.elapsed_time(e1) / args.sweep_steps
-                print(json.dumps({"sweep": "mass_apply_storage", "storage": name, "P": Pp, "Q": Qq, "num_comp": nc,
+                print(json.dumps({"sweep": "mass_apply_storage", "storage": name, "dim": dim, "P": Pp, "Q": Qq,
+                                  "num_comp": nc,
                                   "dofs": nc * N, "ms_per_apply": ms, "gdofs": nc * N / ms / 1e6,
                                   "algorithmic_bytes": ab, "roofline_frac": ab / (ms * 1e-3) / 1e9 / peak}),
                       flush=True)
@@ -384,13 +388,14 @@ def run_sweep(args):
             ev[1].record()
             torch.cuda.synchronize()
             ams = ev[0].elapsed_time(ev[1]) / args.sweep_steps
-            print(json.dumps({"sweep": "mass_apply_auto", "P": Pp, "Q": Qq, "num_comp": nc, "dofs": nc * N,
+            print(json.dumps({"sweep": "mass_apply_auto", "dim": dim, "P": Pp, "Q": Qq, "num_comp": nc,
+                              "dofs": nc * N,
                               "kernel": op.info()["kernel"], "ms_per_apply": ams,
                               "gdofs": nc * N / ams / 1e6}), flush=True)
             del op, ru, qd, u, v
             # standalone basis applies on E-vector / Q-vector sized arrays
             pn, qn = nc * Pp**3 * ne, nc * Qq**3 * ne
-            if nc == 1:
+            if nc == 1 and dim == 3:
                 b = fem.Basis(3, nc, Pp, Qq)
                 for name, t_mode, ev_mode, n_in, n_out, flop_mult in [
                         ("interp", 0, 1, pn, qn, 1), ("interpT", 1, 1, qn, pn, 1),
@@ -881,6 +886,7 @@ def main():
     ap.add_argument("--kernel", choices=["auto", "simple", "pipelined", "paired", "prefetch", "occupancy", "narrow", "element"], default="auto")
     ap.add_argument("--sweep", action="store_true", help="order sweep P=2..8, num_comp 1 and 3 (extra lines)")
     ap.add_argument("--sweep-P", default="2,3,4,5,6,7,8")
+    ap.add_argument("--sweep-dim", default="3", help="dimensions of the order sweep, e.g. 2,3")
     ap.add_argument("--sweep-steps", type=int, default=20)
     ap.add_argument("--solve", action="store_true", help="mixed-precision mass solve, FP64 vs FP32+IR (extra lines)")
     ap.add_argument("--solve-shape", default="64,64,64")

@@ -33,21 +33,33 @@ void set_last_error(const std::string& msg) { g_last_error = msg; }
 // The simple kernel's register policy: no minimum of resident CTAs (ptxas'
 // own heuristic: 55 registers at P=5 where a minimum of 1 lets it take 72 and
 // lose a resident CTA); at P = 6 two resident 392-thread CTAs (83 registers,
-// 80 B of spills, against one CTA at 98 registers); at P = 8 a minimum of 1,
-// where the heuristic caps a 648-thread CTA at 40 registers and spills 1.4 KB.
+// 80 B of spills, against one CTA at 98 registers); at P = 7 two CTAs and at
+// P = 8 one, with the interpolation matrix read from shared memory
+// (plain_shared_matrix).
 template <int P>
 constexpr int plain_min_blocks() {
-  return P >= 8 ? 1 : P == 6 ? 2 : 0;
+  return P >= 8 ? 1 : P >= 6 ? 2 : 0;
 }
 
-template <int P, int Q, int MINB = plain_min_blocks<P>()>
+// At P >= 7 the compiler holds all P*Q matrix entries in registers for the
+// whole tile; read from a shared copy at each use instead (SharedB), P = 8
+// keeps 80 registers with 24 B of spills instead of 728 B, P = 7 fits two
+// resident CTAs: 1.69x (P = 8) and 1.34x (P = 7) on 64M-DoF boxes.  Below
+// P = 7 the extra loads cost more than the registers they free (P = 5: 2.3x
+// slower).
+template <int P>
+constexpr bool plain_shared_matrix() {
+  return P >= 7;
+}
+
+template <int P, int Q, int MINB = plain_min_blocks<P>(), bool SB = plain_shared_matrix<P>() && MINB == plain_min_blocks<P>()>
 void launch_apply3(const MassPlan& p, const double* u, double* v, double* ev, cudaStream_t s) {
   using L = Mass3D<P, Q>;
+  const auto kern = mass3d_apply_kernel<P, Q, MINB, double, ApplyPlain, 1, double, SB>;
   static std::atomic<uint64_t> smem_set{0};
-  set_smem(mass3d_apply_kernel<P, Q, MINB>, L::SMEM, smem_set);
-  mass3d_apply_kernel<P, Q, MINB><<<unsigned(p.tiles()), L::NT, L::SMEM, s>>>(
-      make_mat<P, Q>(p.basis), p.offs(), p.qd(), u, v, ev, p.elems(), p.comp_run, p.comp_stride,
-      ApplyPlain{});
+  set_smem(kern, L::SMEM, smem_set);
+  kern<<<unsigned(p.tiles()), L::NT, L::SMEM, s>>>(make_mat<P, Q>(p.basis), p.offs(), p.qd(), u, v, ev, p.elems(),
+                                                   p.comp_run, p.comp_stride, ApplyPlain{});
   FEM_LAUNCH_CHECK();
 }
 
@@ -118,14 +130,17 @@ void launch_apply3_element(const MassPlan& p, const double* u, double* v, double
   FEM_LAUNCH_CHECK();
 }
 
+// dim 2: the interpolation matrix from shared memory at P >= 7, where holding
+// it in registers leaves one resident CTA (145-168 registers): 1.46x at
+// P = 7, 1.15x at P = 8 (16M-node boxes); slower below.
 template <int P, int Q>
 void launch_apply2(const MassPlan& p, const double* u, double* v, double* ev, cudaStream_t s) {
   using L = Mass2D<P, Q>;
+  const auto kern = mass2d_apply_kernel<P, Q, double, ApplyPlain, double, 0, (P >= 7)>;
   static std::atomic<uint64_t> smem_set{0};
-  set_smem(mass2d_apply_kernel<P, Q>, L::SMEM, smem_set);
-  mass2d_apply_kernel<P, Q><<<unsigned(p.tiles()), L::NT, L::SMEM, s>>>(
-      make_mat<P, Q>(p.basis), p.offs(), p.qd(), u, v, ev, p.elems(), p.comp_run, p.comp_stride,
-      ApplyPlain{});
+  set_smem(kern, L::SMEM, smem_set);
+  kern<<<unsigned(p.tiles()), L::NT, L::SMEM, s>>>(make_mat<P, Q>(p.basis), p.offs(), p.qd(), u, v, ev, p.elems(),
+                                                   p.comp_run, p.comp_stride, ApplyPlain{});
   FEM_LAUNCH_CHECK();
 }
 
@@ -250,13 +265,13 @@ ApplyLauncher variant_launcher(const MassPlan& p, int variant) {
 // one-tile kernel on every B200 of the order sweep (64M-DoF box meshes,
 // Q = P + 1, one and three components), that one; else the one-tile kernel.
 // element at P <= 3 (P = 2: 2.5x, P = 3: 1.1-1.15x), prefetch at P = 7
-// (1.2-1.35x), narrow at P = 8 (1.5x).  Other orders and quadratures: their
-// best variant moves from box to box, which the autotuner settles.
+// (level with the shared-matrix one-tile kernel for one component, 1.1x for
+// three).  Other orders and quadratures: their best variant moves from box to
+// box, which the autotuner settles.
 int default_variant(const MassPlan& p) {
   if (p.dim != 3 || p.Q != p.P + 1) return FEM_B200_KERNEL_SIMPLE;
   if (p.P <= 3) return FEM_B200_KERNEL_ELEMENT;
   if (p.P == 7) return FEM_B200_KERNEL_PREFETCH;
-  if (p.P == 8) return FEM_B200_KERNEL_NARROW;
   return FEM_B200_KERNEL_SIMPLE;
 }
 

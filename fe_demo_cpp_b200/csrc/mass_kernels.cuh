@@ -49,6 +49,15 @@ struct Mat1D {
   T W[Q];      // q_weight_1d
 };
 
+// The interpolation matrix read from a shared-memory copy at every use (the
+// volatile read keeps the compiler from holding all P*Q entries in registers
+// for the whole tile, which at high order costs resident CTAs).  Same values
+// and arithmetic order as reading Mat1D::B, so the same results to the bit.
+template <class T>
+struct SharedB {
+  const volatile T* B;
+};
+
 // Shared-memory plane stride for a tile of 8 elements: an odd multiple of 8
 // doubles, so two adjacent columns of a half-warp land 8 doubles (16 banks)
 // apart.  Tiles of >= 16 elements need no padding (a half-warp is one column).
@@ -117,8 +126,8 @@ struct Mass3D {
 
 // One 8-element tile of the 3D fused apply (the body of mass3d_apply_kernel and
 // of the batched kernels): sa / sb are the CTA's shared buffers A and B.
-template <int P, int Q, class T, class Ext, int NCB, class S = T>
-__device__ __forceinline__ void mass3d_tile(const Mat1D<P, Q, T>& m, T* __restrict__ sa, T* __restrict__ sb,
+template <int P, int Q, class T, class Ext, int NCB, class S = T, class M = Mat1D<P, Q, T>>
+__device__ __forceinline__ void mass3d_tile(const M& m, T* __restrict__ sa, T* __restrict__ sb,
                                             const int* __restrict__ offs, const S* __restrict__ qd,
                                             const S* __restrict__ u, T* __restrict__ v, T* __restrict__ ev,
                                             int num_elem, int num_comp_run, int64_t comp_stride,
@@ -271,8 +280,11 @@ __device__ __forceinline__ void mass3d_tile(const Mat1D<P, Q, T>& m, T* __restri
 // kernel is persistent (tiles blockIdx.x, +gridDim.x, ...) so that each CTA
 // reduces once.  NCB > 1 runs NCB components through each phase together
 // (num_comp_run a multiple of NCB, shared memory NCB * (SA + SB)): more loads
-// in flight and a third of the barriers for a 3-component field.
-template <int P, int Q, int MINB = 1, class T = double, class Ext = ApplyPlain, int NCB = 1, class S = T>
+// in flight and a third of the barriers for a 3-component field.  SB: the
+// contractions read the interpolation matrix from a shared-memory copy
+// (SharedB) instead of the kernel parameter.
+template <int P, int Q, int MINB = 1, class T = double, class Ext = ApplyPlain, int NCB = 1, class S = T,
+          bool SB = false>
 __global__ void __launch_bounds__(Mass3D<P, Q>::NT, MINB) mass3d_apply_kernel(
     const __grid_constant__ Mat1D<P, Q, T> m, const int* __restrict__ offs, const S* __restrict__ qd,
     const S* __restrict__ u, T* __restrict__ v, T* __restrict__ ev, int num_elem, int num_comp_run,
@@ -286,17 +298,26 @@ __global__ void __launch_bounds__(Mass3D<P, Q>::NT, MINB) mass3d_apply_kernel(
     if (ext.st->done) return;  // uniform: the solve has stopped
   }
   double dsum = 0.0;
-
-  if constexpr (Ext::kDot) {  // persistent: one reduction per CTA
-    const int64_t n_tiles = (int64_t(num_elem) + E - 1) / E;
-    for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x)
-      mass3d_tile<P, Q, T, Ext, NCB, S>(m, sa, sb, offs, qd, u, v, ev, num_elem, num_comp_run, comp_stride, ext, tile,
-                                     dsum);
-    double dv[1] = {dsum};
-    grid_sum<1>(dv, ext.part, &ext.st->ticket, [&](const double* tot) { cg_after_apply(ext.st, tot[0]); });
+  auto run = [&](const auto& mat) {
+    if constexpr (Ext::kDot) {  // persistent: one reduction per CTA
+      const int64_t n_tiles = (int64_t(num_elem) + E - 1) / E;
+      for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x)
+        mass3d_tile<P, Q, T, Ext, NCB, S>(mat, sa, sb, offs, qd, u, v, ev, num_elem, num_comp_run, comp_stride, ext,
+                                          tile, dsum);
+      double dv[1] = {dsum};
+      grid_sum<1>(dv, ext.part, &ext.st->ticket, [&](const double* tot) { cg_after_apply(ext.st, tot[0]); });
+    } else {
+      mass3d_tile<P, Q, T, Ext, NCB, S>(mat, sa, sb, offs, qd, u, v, ev, num_elem, num_comp_run, comp_stride, ext,
+                                        blockIdx.x, dsum);
+    }
+  };
+  if constexpr (SB) {
+    __shared__ T b_s[P * Q];
+    for (int i = threadIdx.x; i < P * Q; i += blockDim.x) b_s[i] = m.B[i];
+    __syncthreads();
+    run(SharedB<T>{b_s});
   } else {
-    mass3d_tile<P, Q, T, Ext, NCB, S>(m, sa, sb, offs, qd, u, v, ev, num_elem, num_comp_run, comp_stride, ext,
-                                      blockIdx.x, dsum);
+    run(m);
   }
 }
 
@@ -434,8 +455,8 @@ struct Mass2D {
 };
 
 // One 32-element tile of the 2D fused apply: s1 / s3 the CTA's shared buffers.
-template <int P, int Q, class T, class Ext, class S = T>
-__device__ __forceinline__ void mass2d_tile(const Mat1D<P, Q, T>& m, T* __restrict__ s1, T* __restrict__ s3,
+template <int P, int Q, class T, class Ext, class S = T, class M = Mat1D<P, Q, T>>
+__device__ __forceinline__ void mass2d_tile(const M& m, T* __restrict__ s1, T* __restrict__ s3,
                                             const int* __restrict__ offs, const S* __restrict__ qd,
                                             const S* __restrict__ u, T* __restrict__ v, T* __restrict__ ev,
                                             int num_elem, int num_comp_run, int64_t comp_stride,
@@ -519,8 +540,10 @@ __device__ __forceinline__ void mass2d_tile(const Mat1D<P, Q, T>& m, T* __restri
   }
 }
 
-template <int P, int Q, class T = double, class Ext = ApplyPlain, class S = T>
-__global__ void __launch_bounds__(Mass2D<P, Q>::NT) mass2d_apply_kernel(
+// SB: the contractions read the interpolation matrix from a shared-memory
+// copy (SharedB) instead of the kernel parameter.
+template <int P, int Q, class T = double, class Ext = ApplyPlain, class S = T, int MINB = 0, bool SB = false>
+__global__ void __launch_bounds__(Mass2D<P, Q>::NT, MINB) mass2d_apply_kernel(
     const __grid_constant__ Mat1D<P, Q, T> m, const int* __restrict__ offs, const S* __restrict__ qd,
     const S* __restrict__ u, T* __restrict__ v, T* __restrict__ ev, int num_elem, int num_comp_run,
     int64_t comp_stride, const Ext ext) {
@@ -533,16 +556,26 @@ __global__ void __launch_bounds__(Mass2D<P, Q>::NT) mass2d_apply_kernel(
     if (ext.st->done) return;
   }
   double dsum = 0.0;
-  if constexpr (Ext::kDot) {  // persistent, one reduction per CTA
-    const int64_t n_tiles = (int64_t(num_elem) + E - 1) / E;
-    for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x)
-      mass2d_tile<P, Q, T, Ext, S>(m, s1, s3, offs, qd, u, v, ev, num_elem, num_comp_run, comp_stride, ext, tile,
-                                   dsum);
-    double dv[1] = {dsum};
-    grid_sum<1>(dv, ext.part, &ext.st->ticket, [&](const double* tot) { cg_after_apply(ext.st, tot[0]); });
+  auto run = [&](const auto& mat) {
+    if constexpr (Ext::kDot) {  // persistent, one reduction per CTA
+      const int64_t n_tiles = (int64_t(num_elem) + E - 1) / E;
+      for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x)
+        mass2d_tile<P, Q, T, Ext, S>(mat, s1, s3, offs, qd, u, v, ev, num_elem, num_comp_run, comp_stride, ext,
+                                     tile, dsum);
+      double dv[1] = {dsum};
+      grid_sum<1>(dv, ext.part, &ext.st->ticket, [&](const double* tot) { cg_after_apply(ext.st, tot[0]); });
+    } else {
+      mass2d_tile<P, Q, T, Ext, S>(mat, s1, s3, offs, qd, u, v, ev, num_elem, num_comp_run, comp_stride, ext,
+                                   blockIdx.x, dsum);
+    }
+  };
+  if constexpr (SB) {
+    __shared__ T b_s[P * Q];
+    for (int i = threadIdx.x; i < P * Q; i += blockDim.x) b_s[i] = m.B[i];
+    __syncthreads();
+    run(SharedB<T>{b_s});
   } else {
-    mass2d_tile<P, Q, T, Ext, S>(m, s1, s3, offs, qd, u, v, ev, num_elem, num_comp_run, comp_stride, ext,
-                                 blockIdx.x, dsum);
+    run(m);
   }
 }
 
