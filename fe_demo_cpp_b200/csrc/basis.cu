@@ -12,15 +12,25 @@ namespace {
 
 using BasisLauncher = void (*)(const BasisData&, int, const double*, double*, cudaStream_t);
 
+// Which kernels read the 1D matrices from a shared copy (SharedBG) instead of
+// the parameter, where that beat the parameter on a B200: interp and interp^T
+// from P = 6 (1.2-1.5x; at P = 8 interp 5.7x, the parameter form spilled 656
+// B), grad from P = 5 (1.1-2.3x).  grad^T never gained (0.7-1.0x).
+template <int P, int MODE>
+constexpr bool basis_shared_matrix() {
+  return MODE <= 1 ? P >= 6 : MODE == 2 ? P >= 5 : false;
+}
+
 // MODE: 0 interp, 1 interp^T, 2 grad, 3 grad^T
 template <int P, int Q, int MODE>
 void launch_basis3(const BasisData& b, int ne, const double* u, double* v, cudaStream_t s) {
   using L = Basis3D<P, Q>;
   constexpr int smem = 8 * (MODE <= 1 ? L::SMEM_INTERP : MODE == 2 ? L::SMEM_GRAD_N : L::SMEM_GRAD_T);
-  const auto kern = MODE == 0   ? basis3d_interp_kernel<P, Q>
-                    : MODE == 1 ? basis3d_interp_t_kernel<P, Q>
-                    : MODE == 2 ? basis3d_grad_kernel<P, Q>
-                                : basis3d_grad_t_kernel<P, Q>;
+  constexpr bool SB = basis_shared_matrix<P, MODE>();
+  const auto kern = MODE == 0   ? basis3d_interp_kernel<P, Q, SB>
+                    : MODE == 1 ? basis3d_interp_t_kernel<P, Q, SB>
+                    : MODE == 2 ? basis3d_grad_kernel<P, Q, SB>
+                                : basis3d_grad_t_kernel<P, Q, SB>;
   static std::atomic<uint64_t> smem_set{0};
   set_smem(kern, smem, smem_set);
   const unsigned grid = unsigned((int64_t(ne) + L::E - 1) / L::E);
@@ -38,11 +48,9 @@ template <int P, int DQ, int MODE>
 void fill_one(BasisDispatch& d) {
   constexpr int Q = P + DQ;
   using L = Basis3D<P, Q>;
-  constexpr int smem = 8 * (MODE <= 1 ? L::SMEM_INTERP : MODE == 2 ? L::SMEM_GRAD_N : L::SMEM_GRAD_T);
-  // interp NoTranspose at Q >= 9 (648-thread CTAs) spills 1.2 KB a thread and
-  // measures slower than the generic passes: those keep the generic path
-  constexpr bool slow = MODE == 0 && Q >= 9;
-  if constexpr (smem <= kMaxSmemPerCta && L::NT <= 1024 && !slow) d.fn[P][DQ][MODE] = launch_basis3<P, Q, MODE>;
+  constexpr int smem = 8 * (MODE <= 1 ? L::SMEM_INTERP : MODE == 2 ? L::SMEM_GRAD_N : L::SMEM_GRAD_T) +
+                       (basis_shared_matrix<P, MODE>() ? 16 * P * Q : 0);
+  if constexpr (smem <= kMaxSmemPerCta && L::NT <= 1024) d.fn[P][DQ][MODE] = launch_basis3<P, Q, MODE>;
 }
 
 template <int P, int DQ>

@@ -43,12 +43,34 @@ struct Basis3D {
   static constexpr int MINB_GRAD = 65536 / (2 * NT) >= 96 ? 2 : 1;
 };
 
+// The 1D matrices read from a shared-memory copy at every use (like SharedB):
+// at high order the compiler would hold all 2*P*Q entries in registers.
+struct SharedBG {
+  const volatile double* B;
+  const volatile double* G;
+};
+
+// Runs body(m) with m the kernel's matrix parameter or (SB) a shared copy of
+// its B and G made by the whole CTA.
+template <bool SB, int P, int Q, class F>
+__device__ __forceinline__ void with_matrix(const Mat1D<P, Q>& mp, F&& body) {
+  if constexpr (SB) {
+    __shared__ double bg[2 * P * Q];
+    for (int i = threadIdx.x; i < 2 * P * Q; i += blockDim.x) bg[i] = i < P * Q ? mp.B[i] : mp.G[i - P * Q];
+    __syncthreads();
+    body(SharedBG{bg, bg + P * Q});
+  } else {
+    body(mp);
+  }
+}
+
 // v[k][q][e] = (B x B x B) u[k][i][e]
-template <int P, int Q>
-__global__ void __launch_bounds__(Basis3D<P, Q>::NT) basis3d_interp_kernel(const __grid_constant__ Mat1D<P, Q> m,
+template <int P, int Q, bool SB = false>
+__global__ void __launch_bounds__(Basis3D<P, Q>::NT) basis3d_interp_kernel(const __grid_constant__ Mat1D<P, Q> mp,
                                                                           const double* __restrict__ u,
                                                                           double* __restrict__ v, int num_elem,
                                                                           int num_comp) {
+  with_matrix<SB>(mp, [&](const auto& m) {
   using L = Basis3D<P, Q>;
   constexpr int E = L::E;
   extern __shared__ __align__(16) double smem[];
@@ -104,14 +126,16 @@ __global__ void __launch_bounds__(Basis3D<P, Q>::NT) basis3d_interp_kernel(const
     // the next component's A writes sa, last read by B before the barrier
     // above; its B writes sb after its own barrier, which every C has passed
   }
+  });
 }
 
 // v[k][i][e] = (B^T x B^T x B^T) u[k][q][e]
-template <int P, int Q>
-__global__ void __launch_bounds__(Basis3D<P, Q>::NT) basis3d_interp_t_kernel(const __grid_constant__ Mat1D<P, Q> m,
+template <int P, int Q, bool SB = false>
+__global__ void __launch_bounds__(Basis3D<P, Q>::NT) basis3d_interp_t_kernel(const __grid_constant__ Mat1D<P, Q> mp,
                                                                             const double* __restrict__ u,
                                                                             double* __restrict__ v, int num_elem,
                                                                             int num_comp) {
+  with_matrix<SB>(mp, [&](const auto& m) {
   using L = Basis3D<P, Q>;
   constexpr int E = L::E;
   extern __shared__ __align__(16) double smem[];
@@ -163,14 +187,16 @@ __global__ void __launch_bounds__(Basis3D<P, Q>::NT) basis3d_interp_t_kernel(con
       }
     }
   }
+  });
 }
 
 // v[d][k][q][e] = d/dX_d of u[k][i][e] at the points (G on axis d, B on the others)
-template <int P, int Q>
-__global__ void __launch_bounds__(Basis3D<P, Q>::NT, Basis3D<P, Q>::MINB_GRAD) basis3d_grad_kernel(const __grid_constant__ Mat1D<P, Q> m,
+template <int P, int Q, bool SB = false>
+__global__ void __launch_bounds__(Basis3D<P, Q>::NT, Basis3D<P, Q>::MINB_GRAD) basis3d_grad_kernel(const __grid_constant__ Mat1D<P, Q> mp,
                                                                         const double* __restrict__ u,
                                                                         double* __restrict__ v, int num_elem,
                                                                         int num_comp) {
+  with_matrix<SB>(mp, [&](const auto& m) {
   using L = Basis3D<P, Q>;
   constexpr int E = L::E;
   extern __shared__ __align__(16) double smem[];
@@ -239,7 +265,7 @@ __global__ void __launch_bounds__(Basis3D<P, Q>::NT, Basis3D<P, Q>::MINB_GRAD) b
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
         const double* src = d == 0 ? sbb : d == 1 ? sgb : sbg;
-        const double* mx = d == 0 ? m.G : m.B;  // d/dx contracts x with G
+        const auto mx = d == 0 ? m.G : m.B;  // d/dx contracts x with G
         double w[P];
 #pragma unroll
         for (int px = 0; px < P; ++px) w[px] = src[px * L::PS2 + col * E + e];
@@ -253,14 +279,16 @@ __global__ void __launch_bounds__(Basis3D<P, Q>::NT, Basis3D<P, Q>::MINB_GRAD) b
       }
     }
   }
+  });
 }
 
 // v[k][i][e] = sum_d (d/dX_d)^T u[d][k][q][e]
-template <int P, int Q>
-__global__ void __launch_bounds__(Basis3D<P, Q>::NT, Basis3D<P, Q>::MINB_GRAD) basis3d_grad_t_kernel(const __grid_constant__ Mat1D<P, Q> m,
+template <int P, int Q, bool SB = false>
+__global__ void __launch_bounds__(Basis3D<P, Q>::NT, Basis3D<P, Q>::MINB_GRAD) basis3d_grad_t_kernel(const __grid_constant__ Mat1D<P, Q> mp,
                                                                           const double* __restrict__ u,
                                                                           double* __restrict__ v, int num_elem,
                                                                           int num_comp) {
+  with_matrix<SB>(mp, [&](const auto& m) {
   using L = Basis3D<P, Q>;
   constexpr int E = L::E;
   extern __shared__ __align__(16) double smem[];
@@ -336,6 +364,7 @@ __global__ void __launch_bounds__(Basis3D<P, Q>::NT, Basis3D<P, Q>::MINB_GRAD) b
     }
     __syncthreads();  // the next component's C^T rewrites s0..s2 (read by F) and F rewrites sa, sz (read by G)
   }
+  });
 }
 
 }  // namespace fem_b200
