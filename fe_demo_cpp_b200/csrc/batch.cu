@@ -53,6 +53,27 @@ __global__ void batch_to_float_kernel(int64_t n, const double* __restrict__ in, 
 }
 
 // Tiles g = blockIdx.x, +gridDim.x, ... of a class; tiles[g] = (mesh, tile).
+// FP64 classes of P >= 7 read the 1D matrix from a shared copy (SharedB), as
+// the single-mesh one-tile kernels do: the parameter form holds all P*Q
+// entries in registers and keeps one resident CTA.
+template <int P, class T>
+constexpr bool batch_shared_matrix() {
+  return P >= 7 && sizeof(T) == 8;
+}
+
+// Runs body(m) with m the matrix parameter or (SB) a CTA-wide shared copy.
+template <bool SB, int P, int Q, class T, class F>
+__device__ __forceinline__ void with_interp(const Mat1D<P, Q, T>& mp, F&& body) {
+  if constexpr (SB) {
+    __shared__ T b_s[P * Q];
+    for (int i = threadIdx.x; i < P * Q; i += blockDim.x) b_s[i] = mp.B[i];
+    __syncthreads();
+    body(SharedB<T>{b_s});
+  } else {
+    body(mp);
+  }
+}
+
 template <int P, int Q, int MINB, class T, int NCB>
 __global__ void __launch_bounds__(Mass3D<P, Q>::NT, MINB)
     mass3d_batch_kernel(const __grid_constant__ Mat1D<P, Q, T> m, const BatchMesh<T>* __restrict__ meshes,
@@ -62,12 +83,14 @@ __global__ void __launch_bounds__(Mass3D<P, Q>::NT, MINB)
   T* sa = reinterpret_cast<T*>(smem_bytes);
   T* sb = sa + NCB * L::SA;
   double dsum = 0.0;
-  for (int64_t g = blockIdx.x; g < n_tiles; g += gridDim.x) {
-    const int2 tm = tiles[g];
-    const BatchMesh<T> mm = meshes[tm.x];
-    mass3d_tile<P, Q, T, ApplyPlain, NCB>(m, sa, sb, mm.offs, mm.qd, mm.u, mm.v, nullptr, mm.num_elem, mm.comp_run,
-                                          mm.comp_stride, ApplyPlain{}, tm.y, dsum);
-  }
+  with_interp<batch_shared_matrix<P, T>()>(m, [&](const auto& mat) {
+    for (int64_t g = blockIdx.x; g < n_tiles; g += gridDim.x) {
+      const int2 tm = tiles[g];
+      const BatchMesh<T> mm = meshes[tm.x];
+      mass3d_tile<P, Q, T, ApplyPlain, NCB>(mat, sa, sb, mm.offs, mm.qd, mm.u, mm.v, nullptr, mm.num_elem,
+                                            mm.comp_run, mm.comp_stride, ApplyPlain{}, tm.y, dsum);
+    }
+  });
 }
 
 template <int P, int Q, class T>
@@ -79,12 +102,14 @@ __global__ void __launch_bounds__(Mass2D<P, Q>::NT)
   T* s1 = reinterpret_cast<T*>(smem_bytes);
   T* s3 = s1 + L::S1;
   double dsum = 0.0;
-  for (int64_t g = blockIdx.x; g < n_tiles; g += gridDim.x) {
-    const int2 tm = tiles[g];
-    const BatchMesh<T> mm = meshes[tm.x];
-    mass2d_tile<P, Q, T, ApplyPlain>(m, s1, s3, mm.offs, mm.qd, mm.u, mm.v, nullptr, mm.num_elem, mm.comp_run,
-                                     mm.comp_stride, ApplyPlain{}, tm.y, dsum);
-  }
+  with_interp<batch_shared_matrix<P, T>()>(m, [&](const auto& mat) {
+    for (int64_t g = blockIdx.x; g < n_tiles; g += gridDim.x) {
+      const int2 tm = tiles[g];
+      const BatchMesh<T> mm = meshes[tm.x];
+      mass2d_tile<P, Q, T, ApplyPlain>(mat, s1, s3, mm.offs, mm.qd, mm.u, mm.v, nullptr, mm.num_elem, mm.comp_run,
+                                       mm.comp_stride, ApplyPlain{}, tm.y, dsum);
+    }
+  });
 }
 
 template <int P, int Q, class T>
@@ -135,9 +160,9 @@ constexpr int kBatchMaxStreams = 4;
 // for P <= 5 (3 with three components batched), 2 for P = 6, 1 above, and
 // no more than leave 56 registers a thread (72 with three components, 80 at
 // P = 6).
-constexpr int batch_min_blocks(int P, int threads, int ncb) {
-  const int cap = P > 6 ? 1 : P == 6 ? 2 : ncb == 3 ? 3 : 4;
-  const int regs = P == 6 ? 80 : ncb == 3 ? 72 : 56;
+constexpr int batch_min_blocks(int P, int threads, int ncb, bool shared_matrix = false) {
+  const int cap = P > 7 ? 1 : P == 7 ? (shared_matrix ? 2 : 1) : P == 6 ? 2 : ncb == 3 ? 3 : 4;
+  const int regs = P == 7 ? 64 : P == 6 ? 80 : ncb == 3 ? 72 : 56;
   for (int b = cap; b > 1; --b)
     if (b * threads <= 2048 && 65536 / (b * threads) >= regs) return b;
   return P >= 8 ? 1 : 0;  // as the single-mesh kernel (plain_min_blocks)
@@ -147,7 +172,7 @@ template <int P, int Q, class T, int NCB>
 unsigned launch_batch3(const BatchClass& c, const void* meshes, unsigned grid, cudaStream_t s) {
   using L = Mass3D<P, Q>;
   constexpr int smem = NCB * (L::SA + L::SB) * int(sizeof(T));
-  constexpr int minb = batch_min_blocks(P, L::NT, NCB);
+  constexpr int minb = batch_min_blocks(P, L::NT, NCB, batch_shared_matrix<P, T>());
   const auto kern = mass3d_batch_kernel<P, Q, minb, T, NCB>;
   static std::atomic<uint64_t> smem_set{0};
   set_smem(kern, smem, smem_set);

@@ -63,7 +63,7 @@ def make_op(fem, cuda, dim, shape, P, Q, nc, qf, seed, interleaved=False):
 
 
 def mixed_batch(fem, cuda):
-    """Uneven members: 1D/2D/3D, P 2..7, Q = P..P+2, 1-3 components, both
+    """Uneven members: 1D/2D/3D, P 2..8, Q = P..P+2, 1-3 components, both
     QFunctions, blocked and interleaved layouts, repeated shapes (so classes
     have several members) and single-element meshes (tail tiles)."""
     V, S = fem.QF.apply_mass_vector, fem.QF.apply_mass
@@ -71,7 +71,9 @@ def mixed_batch(fem, cuda):
             (3, (4, 3, 3), 5, 6, 3, V), (3, (2, 2, 3), 5, 6, 3, V), (3, (3, 3, 2), 3, 4, 2, V),
             (3, (2, 2, 2), 6, 7, 1, S), (3, (2, 1, 2), 7, 9, 1, S), (3, (3, 2, 2), 2, 3, 3, S),
             (2, (7, 5), 3, 4, 1, S), (2, (9, 9), 5, 6, 2, V), (2, (1, 1), 2, 2, 1, S), (2, (12, 7), 3, 4, 1, S),
-            (1, (300,), 4, 5, 1, S), (1, (9,), 3, 5, 2, V)]
+            (1, (300,), 4, 5, 1, S), (1, (9,), 3, 5, 2, V),
+            # high order: the FP64 classes read the 1D matrix from shared memory
+            (3, (2, 2, 1), 8, 9, 1, S), (2, (5, 4), 7, 8, 1, S), (2, (3, 3), 8, 9, 2, V)]
     ops, metas = [], []
     for i, (dim, shape, P, Q, nc, qf) in enumerate(spec):
         op, meta = make_op(fem, cuda, dim, shape, P, Q, nc, qf, seed=i, interleaved=(i % 2 == 1 and nc > 1))
