@@ -337,8 +337,8 @@ void launch_diag(const MassPlan& p, double* diag, double* ev, cudaStream_t s) {
 // orders leave registers to ptxas (0), P = 8 asks for one CTA (see
 // plain_min_blocks in device.cu).
 constexpr int kCgMaxBlocks = 4, kCgMinRegs = 56;
-constexpr int cg_min_blocks(int threads, int P) {
-  if (P > 5) return P >= 8 ? 1 : 0;
+constexpr int cg_min_blocks(int threads, int P, bool shared_matrix = false) {
+  if (P > 5) return P >= 8 ? 1 : P == 7 && shared_matrix ? 2 : 0;
   for (int b = kCgMaxBlocks; b > 1; --b)
     if (65536 / (b * threads) >= kCgMinRegs && b * threads <= 2048) return b;
   return 1;
@@ -358,7 +358,9 @@ void launch_cg_apply3(const MassPlan& p, const T* r, T* w, T* ev, const T* qd, c
   using L = Mass3D<P, Q>;
   constexpr int smem = NCB * (L::SA + L::SB) * int(sizeof(T));
   static std::atomic<uint64_t> smem_set{0};
-  const auto kern = mass3d_apply_kernel<P, Q, cg_min_blocks(L::NT, P), T, ApplyCg<T>, NCB>;
+  // FP64 at P >= 7: the 1D matrix from a shared copy, as the one-tile apply
+  constexpr bool sb = P >= 7 && sizeof(T) == 8;
+  const auto kern = mass3d_apply_kernel<P, Q, cg_min_blocks(L::NT, P, sb), T, ApplyCg<T>, NCB, T, sb>;
   set_smem(kern, smem, smem_set);
   kern<<<resident_grid(kern, L::NT, smem, p.n_tiles), L::NT, smem, s>>>(
       typed_mat<P, Q, T>(p.basis), p.offs_t.get(), qd, r, w, ev, p.num_elem, p.comp_run, p.comp_stride, ext);

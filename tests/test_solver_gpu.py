@@ -71,7 +71,7 @@ def operator(fem, cuda, m, Q, nc=1, interleaved=False, scatter=0):
 
 
 CASES = [(1, (9,), 4, 5, 1), (2, (4, 3), 3, 4, 1), (2, (3, 3), 5, 6, 2), (3, (2, 2, 2), 3, 4, 1),
-         (3, (3, 2, 2), 4, 5, 3), (3, (2, 2, 1), 6, 7, 1)]
+         (3, (3, 2, 2), 4, 5, 3), (3, (2, 2, 1), 6, 7, 1), (3, (2, 1, 1), 7, 8, 1), (3, (1, 1, 1), 8, 9, 1)]
 
 
 @pytest.mark.parametrize("dim,shape,P,Q,nc", CASES)
