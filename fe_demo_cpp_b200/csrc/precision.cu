@@ -50,8 +50,9 @@ void launch_lowp(const MassPlan& p, const S* qd, const S* u, float* v, float* ev
     const auto kern = mass3d_apply_kernel<P, Q, lowp_min_blocks<P>(), float, ApplyPlain, 1, S>;
     static std::atomic<uint64_t> smem_set{0};
     set_smem(kern, smem, smem_set);
+    const int64_t wave = resident_ctas(reinterpret_cast<const void*>(kern), L::NT, smem);  // L2 prefetch distance
     kern<<<unsigned(p.n_tiles), L::NT, smem, s>>>(f32_mat<P, Q>(p.basis), p.offs_t.get(), qd, u, v, ev, p.num_elem,
-                                                  p.comp_run, p.comp_stride, ApplyPlain{});
+                                                  p.comp_run, p.comp_stride, ApplyPlain{}, wave);
   } else if (p.dim == 2) {
     using L = Mass2D<P, Q>;
     constexpr int smem = (L::S1 + L::S3) * 4;

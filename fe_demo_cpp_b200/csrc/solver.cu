@@ -363,7 +363,7 @@ void launch_cg_apply3(const MassPlan& p, const T* r, T* w, T* ev, const T* qd, c
   const auto kern = mass3d_apply_kernel<P, Q, cg_min_blocks(L::NT, P, sb), T, ApplyCg<T>, NCB, T, sb>;
   set_smem(kern, smem, smem_set);
   kern<<<resident_grid(kern, L::NT, smem, p.n_tiles), L::NT, smem, s>>>(
-      typed_mat<P, Q, T>(p.basis), p.offs_t.get(), qd, r, w, ev, p.num_elem, p.comp_run, p.comp_stride, ext);
+      typed_mat<P, Q, T>(p.basis), p.offs_t.get(), qd, r, w, ev, p.num_elem, p.comp_run, p.comp_stride, ext, 0);
   FEM_LAUNCH_CHECK();
 }
 
