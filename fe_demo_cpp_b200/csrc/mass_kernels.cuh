@@ -302,7 +302,8 @@ __device__ __forceinline__ void mass3d_tile(const M& m, T* __restrict__ sa, T* _
 // (SharedB) instead of the kernel parameter.  l2_ahead > 0 (one CTA per tile):
 // CTA b first has the qdata and offsets of tile b + l2_ahead prefetched into
 // L2, so that the CTA which takes that tile about a wave later finds them
-// there instead of waiting on DRAM (P = 5: 1.05x sustained).
+// there instead of waiting on DRAM (P = 5: 1.05x sustained); persistent (Ext
+// with a reduction), l2_ahead != 0: each CTA prefetches its next tile.
 template <int P, int Q, int MINB = 1, class T = double, class Ext = ApplyPlain, int NCB = 1, class S = T,
           bool SB = false>
 __global__ void __launch_bounds__(Mass3D<P, Q>::NT, MINB) mass3d_apply_kernel(
@@ -326,9 +327,13 @@ __global__ void __launch_bounds__(Mass3D<P, Q>::NT, MINB) mass3d_apply_kernel(
   auto run = [&](const auto& mat) {
     if constexpr (Ext::kDot) {  // persistent: one reduction per CTA
       const int64_t n_tiles = (int64_t(num_elem) + E - 1) / E;
-      for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x)
+      for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+        // l2_ahead != 0: this CTA's next tile (a wave ahead) into L2 first
+        if (l2_ahead != 0 && threadIdx.x == 0 && tile + gridDim.x < n_tiles)
+          prefetch_tile_l2<L::ES, L::NQ, E, S>(offs, qd, tile + gridDim.x);
         mass3d_tile<P, Q, T, Ext, NCB, S>(mat, sa, sb, offs, qd, u, v, ev, num_elem, num_comp_run, comp_stride, ext,
                                           tile, dsum);
+      }
       double dv[1] = {dsum};
       grid_sum<1>(dv, ext.part, &ext.st->ticket, [&](const double* tot) { cg_after_apply(ext.st, tot[0]); });
     } else {
