@@ -131,8 +131,12 @@ void launch_apply3_narrow(const MassPlan& p, const double* u, double* v, double*
 template <int P, int Q>
 void launch_apply3_element(const MassPlan& p, const double* u, double* v, double* ev, cudaStream_t s) {
   const unsigned grid = unsigned((p.tiles() * 8 + 127) / 128);
-  mass3d_apply_element_kernel<P, Q><<<grid, 128, 0, s>>>(make_mat<P, Q>(p.basis), p.offs(), p.qd(), u,
-                                                          v, ev, p.elems(), p.comp_run, p.comp_stride);
+  const auto kern = mass3d_apply_element_kernel<P, Q>;
+  // L2 prefetch a wave ahead at P = 3 (1.05-1.07x); at P = 2 it measured
+  // slightly slower (0.98x) and stays off
+  const int64_t wave = P == 3 ? resident_ctas(reinterpret_cast<const void*>(kern), 128, 0) : 0;
+  kern<<<grid, 128, 0, s>>>(make_mat<P, Q>(p.basis), p.offs(), p.qd(), u, v, ev, p.elems(), p.comp_run,
+                            p.comp_stride, wave);
   FEM_LAUNCH_CHECK();
 }
 
@@ -145,8 +149,11 @@ void launch_apply2(const MassPlan& p, const double* u, double* v, double* ev, cu
   const auto kern = mass2d_apply_kernel<P, Q, double, ApplyPlain, double, 0, (P >= 7)>;
   static std::atomic<uint64_t> smem_set{0};
   set_smem(kern, L::SMEM, smem_set);
+  // L2 prefetch a wave ahead at P <= 4 (P = 2, 3: 1.10-1.12x one component,
+  // 1.03-1.04x three); neutral at P = 5, so off from there
+  const int64_t wave = P <= 4 ? resident_ctas(reinterpret_cast<const void*>(kern), L::NT, L::SMEM) : 0;
   kern<<<unsigned(p.tiles()), L::NT, L::SMEM, s>>>(make_mat<P, Q>(p.basis), p.offs(), p.qd(), u, v, ev, p.elems(),
-                                                   p.comp_run, p.comp_stride, ApplyPlain{});
+                                                   p.comp_run, p.comp_stride, ApplyPlain{}, wave);
   FEM_LAUNCH_CHECK();
 }
 

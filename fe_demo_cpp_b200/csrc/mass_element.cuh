@@ -17,6 +17,8 @@
 
 namespace fem_b200 {
 
+// l2_ahead > 0: the first warp of CTA b has the qdata and offsets of CTA
+// b + l2_ahead's 16 tiles prefetched into L2 (one lane a block).
 template <int P, int Q>
 __global__ void __launch_bounds__(128) mass3d_apply_element_kernel(const __grid_constant__ Mat1D<P, Q> m,
                                                                   const int* __restrict__ offs,
@@ -24,8 +26,18 @@ __global__ void __launch_bounds__(128) mass3d_apply_element_kernel(const __grid_
                                                                   const double* __restrict__ u,
                                                                   double* __restrict__ v, double* __restrict__ ev,
                                                                   int num_elem, int num_comp_run,
-                                                                  int64_t comp_stride) {
+                                                                  int64_t comp_stride, int64_t l2_ahead = 0) {
   constexpr int TE = 8, ES = P * P * P, NQ = Q * Q * Q;
+  if (l2_ahead > 0 && threadIdx.x < 32) {
+    const int64_t n_tiles = (int64_t(num_elem) + TE - 1) / TE;
+    const int64_t t = (int64_t(blockIdx.x) + l2_ahead) * (128 / TE) + (threadIdx.x & 15);
+    if (t < n_tiles) {
+      if (threadIdx.x < 16)
+        l2_prefetch_bulk(qd + t * (int64_t(NQ) * TE), unsigned(NQ * TE * 8));
+      else
+        l2_prefetch_bulk(offs + t * (int64_t(ES) * TE), unsigned(ES * TE * 4));
+    }
+  }
   const int64_t eg = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (eg >= num_elem) return;
   const int64_t tile = eg / TE;

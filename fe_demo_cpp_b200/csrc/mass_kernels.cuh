@@ -133,7 +133,7 @@ __device__ __forceinline__ void l2_prefetch_bulk(const void* p, unsigned bytes) 
 // One thread's L2 prefetch of a tile's qdata and offsets blocks, laid out
 // [tile][...][e] (NQ * E values and ES * E offsets a tile).  Each block
 // starts at a multiple of its size from a 256-byte aligned allocation, and
-// both sizes are multiples of 16 bytes (E = 8: 8 * NQ * sizeof(S), 32 * ES).
+// both sizes are multiples of 16 bytes (E = 8 or 32 elements a tile).
 template <int ES, int NQ, int E, class S>
 __device__ __forceinline__ void prefetch_tile_l2(const int* offs, const S* qd, int64_t tile) {
   static_assert((NQ * E * sizeof(S)) % 16 == 0 && (ES * E * 4) % 16 == 0, "bulk prefetch sizes");
@@ -571,12 +571,14 @@ __device__ __forceinline__ void mass2d_tile(const M& m, T* __restrict__ s1, T* _
 }
 
 // SB: the contractions read the interpolation matrix from a shared-memory
-// copy (SharedB) instead of the kernel parameter.
+// copy (SharedB) instead of the kernel parameter.  l2_ahead > 0 (one CTA per
+// tile): CTA b has tile b + l2_ahead's qdata and offsets prefetched into L2,
+// as the 3D kernel.
 template <int P, int Q, class T = double, class Ext = ApplyPlain, class S = T, int MINB = 0, bool SB = false>
 __global__ void __launch_bounds__(Mass2D<P, Q>::NT, MINB) mass2d_apply_kernel(
     const __grid_constant__ Mat1D<P, Q, T> m, const int* __restrict__ offs, const S* __restrict__ qd,
     const S* __restrict__ u, T* __restrict__ v, T* __restrict__ ev, int num_elem, int num_comp_run,
-    int64_t comp_stride, const Ext ext) {
+    int64_t comp_stride, const Ext ext, int64_t l2_ahead = 0) {
   using L = Mass2D<P, Q>;
   constexpr int E = L::E;
   extern __shared__ __align__(16) unsigned char smem_bytes[];
@@ -584,6 +586,11 @@ __global__ void __launch_bounds__(Mass2D<P, Q>::NT, MINB) mass2d_apply_kernel(
   T* s3 = s1 + L::S1;
   if constexpr (Ext::kDot) {
     if (ext.st->done) return;
+  }
+  if constexpr (!Ext::kDot) {
+    const int64_t ahead = blockIdx.x + l2_ahead;
+    if (l2_ahead > 0 && threadIdx.x == 0 && ahead < (int64_t(num_elem) + E - 1) / E)
+      prefetch_tile_l2<L::ES, L::NQ, E, S>(offs, qd, ahead);
   }
   double dsum = 0.0;
   auto run = [&](const auto& mat) {

@@ -59,8 +59,9 @@ void launch_lowp(const MassPlan& p, const S* qd, const S* u, float* v, float* ev
     const auto kern = mass2d_apply_kernel<P, Q, float, ApplyPlain, S>;
     static std::atomic<uint64_t> smem_set{0};
     set_smem(kern, smem, smem_set);
+    // no L2 prefetch in 2D reduced storage: measured mixed (BF16 at P = 2: 0.85-0.88x)
     kern<<<unsigned(p.n_tiles), L::NT, smem, s>>>(f32_mat<P, Q>(p.basis), p.offs_t.get(), qd, u, v, ev, p.num_elem,
-                                                  p.comp_run, p.comp_stride, ApplyPlain{});
+                                                  p.comp_run, p.comp_stride, ApplyPlain{}, 0);
   } else {
     mass1d_apply_kernel<P, Q, float, ApplyPlain, S><<<unsigned(p.n_tiles), 128, 0, s>>>(
         f32_mat<P, Q>(p.basis), p.offs_t.get(), qd, u, v, ev, p.num_elem, p.comp_run, p.comp_stride, ApplyPlain{});

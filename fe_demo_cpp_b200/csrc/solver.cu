@@ -391,7 +391,7 @@ void launch_cg_apply(const MassPlan& p, const T* r, T* w, T* ev, const T* qd, co
     const auto kern = mass2d_apply_kernel<P, Q, T, ApplyCg<T>>;
     set_smem(kern, smem, smem_set);
     kern<<<resident_grid(kern, L::NT, smem, p.n_tiles), L::NT, smem, s>>>(
-        typed_mat<P, Q, T>(p.basis), p.offs_t.get(), qd, r, w, ev, p.num_elem, p.comp_run, p.comp_stride, ext);
+        typed_mat<P, Q, T>(p.basis), p.offs_t.get(), qd, r, w, ev, p.num_elem, p.comp_run, p.comp_stride, ext, 0);
   } else {
     const auto kern = mass1d_apply_kernel<P, Q, T, ApplyCg<T>>;
     kern<<<resident_grid(kern, 128, 0, p.n_tiles), 128, 0, s>>>(
