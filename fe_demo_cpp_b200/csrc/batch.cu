@@ -416,7 +416,10 @@ int fem_b200_batch_create(const fem_b200_mass* ops, int num_ops, int precision, 
         BatchClass c;
         c.dim = p.dim, c.P = p.P, c.Q = p.Q, c.comp_run = p.comp_run;
         c.basis = p.basis;
-        c.ncb = (p.dim == 3 && p.comp_run == 3 && p.P <= 5 && disp.fn[2][p.P][p.Q - p.P][1][ti]) ? 3 : 1;
+        // three components through each phase together in FP32 only: for FP64
+        // classes one at a time measured faster (512 uneven meshes, one graph:
+        // 58.0 -> 62.1 GDoF/s), as for the FP64 Krylov apply
+        c.ncb = (ti == 1 && p.dim == 3 && p.comp_run == 3 && p.P <= 5 && disp.fn[2][p.P][p.Q - p.P][1][ti]) ? 3 : 1;
         c.launch = disp.fn[p.dim - 1][p.P][p.Q - p.P][c.ncb == 3 ? 1 : 0][ti];
         require(c.launch != nullptr, "batch create: no batched kernel for this shape");
         it = index.emplace(key, int(b->classes.size())).first;

@@ -373,13 +373,15 @@ template <int P, int Q, class T>
 void launch_cg_apply(const MassPlan& p, const T* r, T* w, T* ev, const T* qd, const ApplyCg<T>& ext,
                      cudaStream_t s) {
   if (p.dim == 3) {
-    // components batched through the phases (measured faster for 2 and 3
-    // components in both precisions) where shared memory allows
+    // FP32: components batched through the phases where shared memory allows;
+    // FP64: one at a time.  64^3 hexes, P = 5, 3 components: FP32 solve 32.1
+    // ms batched vs 34.7 ms one at a time; FP64 56.2 ms batched (3 resident
+    // CTAs, shared memory bound) vs 52.1 ms one at a time (4 CTAs).
     constexpr int smem1 = (Mass3D<P, Q>::SA + Mass3D<P, Q>::SB) * int(sizeof(T));
-    if constexpr (3 * smem1 <= kMaxSmemPerCta) {
+    if constexpr (sizeof(T) == 4 && 3 * smem1 <= kMaxSmemPerCta) {
       if (p.comp_run == 3) return launch_cg_apply3<P, Q, T, 3>(p, r, w, ev, qd, ext, s);
     }
-    if constexpr (2 * smem1 <= kMaxSmemPerCta) {
+    if constexpr (sizeof(T) == 4 && 2 * smem1 <= kMaxSmemPerCta) {
       if (p.comp_run == 2) return launch_cg_apply3<P, Q, T, 2>(p, r, w, ev, qd, ext, s);
     }
     return launch_cg_apply3<P, Q, T, 1>(p, r, w, ev, qd, ext, s);
