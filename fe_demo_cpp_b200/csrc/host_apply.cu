@@ -44,16 +44,22 @@
 namespace fem_b200 {
 namespace {
 
-// Block c: the smallest and largest offset of the elements in chunk c
-// (tiled layout [tile][i][e], padding elements excluded).
+// Blocks (c, j): the smallest and largest offset of the elements in slice j
+// of chunk c (tiled layout [tile][i][e], padding elements excluded), folded
+// into lo[c] / hi[c] (set beforehand to INT_MAX-like 0x7f7f7f7f and -1).
+constexpr int kSpanSlices = 64;
+
 __global__ void chunk_span_kernel(const int* __restrict__ offs, int es, int tile_e, int num_elem, int64_t n_tiles,
                                   int64_t tiles_per_chunk, int* __restrict__ lo, int* __restrict__ hi) {
   __shared__ int s_lo, s_hi;
   if (threadIdx.x == 0) s_lo = INT_MAX, s_hi = -1;
   __syncthreads();
   const int64_t per_tile = int64_t(es) * tile_e;
-  const int64_t t0 = int64_t(blockIdx.x) * tiles_per_chunk;
-  const int64_t t1 = t0 + tiles_per_chunk < n_tiles ? t0 + tiles_per_chunk : n_tiles;
+  const int64_t c0 = int64_t(blockIdx.x) * tiles_per_chunk;
+  const int64_t c1 = c0 + tiles_per_chunk < n_tiles ? c0 + tiles_per_chunk : n_tiles;
+  const int64_t step = (c1 - c0 + gridDim.y - 1) / gridDim.y;
+  const int64_t t0 = c0 + blockIdx.y * step;
+  const int64_t t1 = t0 + step < c1 ? t0 + step : c1;
   int mn = INT_MAX, mx = -1;
   for (int64_t pos = t0 * per_tile + threadIdx.x; pos < t1 * per_tile; pos += blockDim.x) {
     const int64_t tile = pos / per_tile;
@@ -67,7 +73,10 @@ __global__ void chunk_span_kernel(const int* __restrict__ offs, int es, int tile
   atomicMin(&s_lo, mn);
   atomicMax(&s_hi, mx);
   __syncthreads();
-  if (threadIdx.x == 0) lo[blockIdx.x] = s_lo, hi[blockIdx.x] = s_hi;
+  if (threadIdx.x == 0 && s_hi >= 0) {
+    atomicMin(lo + blockIdx.x, s_lo);
+    atomicMax(hi + blockIdx.x, s_hi);
+  }
 }
 
 // Chunks: about 24, each at least 512 tiles (a wave of the apply kernel), an
@@ -94,8 +103,10 @@ HostPipeline& pipeline(MassPlan& p, cudaStream_t s) {
   const int64_t n_chunks = (p.n_tiles + tpc - 1) / tpc;
   hp->tiles_per_chunk = tpc;
   DevBuf<int> span(size_t(2 * n_chunks));
-  chunk_span_kernel<<<unsigned(n_chunks), 256, 0, s>>>(p.offs_t.get(), p.es, p.tile_e, p.num_elem, p.n_tiles, tpc,
-                                                       span.get(), span.get() + n_chunks);
+  FEM_CUDA_CHECK(cudaMemsetAsync(span.get(), 0x7f, size_t(n_chunks) * sizeof(int), s));              // lo
+  FEM_CUDA_CHECK(cudaMemsetAsync(span.get() + n_chunks, 0xff, size_t(n_chunks) * sizeof(int), s));  // hi = -1
+  chunk_span_kernel<<<dim3(unsigned(n_chunks), kSpanSlices), 256, 0, s>>>(
+      p.offs_t.get(), p.es, p.tile_e, p.num_elem, p.n_tiles, tpc, span.get(), span.get() + n_chunks);
   FEM_LAUNCH_CHECK();
   std::vector<int> h(size_t(2 * n_chunks));
   FEM_CUDA_CHECK(cudaMemcpyAsync(h.data(), span.get(), h.size() * sizeof(int), cudaMemcpyDeviceToHost, s));
