@@ -136,14 +136,26 @@ bool page_locked(const void* ptr) {
 constexpr int kSlots = 6;
 constexpr int64_t kSlotElems = int64_t(1) << 20;
 
+// The memcpy threads, one pool for the process (half the hardware threads,
+// 2 to 8), shared by every plan's staging; made on first use.
+CopyPool& copy_pool() {
+  static CopyPool pool(int(std::min(8u, std::max(2u, std::thread::hardware_concurrency() / 2))));
+  return pool;
+}
+
 void ensure_staging(HostPipeline& hp) {
-  if (hp.pool) return;
+  if (!hp.slot_ev.empty()) return;
   hp.ring_in.alloc(size_t(kSlots * kSlotElems));
   hp.ring_out.alloc(size_t(kSlots * kSlotElems));
-  hp.slot_ev.assign(size_t(2 * kSlots), nullptr);
-  for (cudaEvent_t& e : hp.slot_ev) FEM_CUDA_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-  const unsigned hw = std::thread::hardware_concurrency();
-  hp.pool = std::make_unique<CopyPool>(int(std::min(8u, std::max(2u, hw / 2))));
+  std::vector<cudaEvent_t> ev(size_t(2 * kSlots), nullptr);
+  for (cudaEvent_t& e : ev) {
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+      for (cudaEvent_t made : ev)
+        if (made) (void)cudaEventDestroy(made);
+      FEM_CUDA_CHECK(cudaGetLastError());
+    }
+  }
+  hp.slot_ev = std::move(ev);
 }
 
 struct Copy {
@@ -293,7 +305,7 @@ void mass_apply_host_pipelined(MassPlan& p, const double* u_host, double* v_host
           for (; issued < out.size() && issued < j + kSlots && recorded(out[issued].chunk, false); ++issued)
             issue(issued);
           FEM_CUDA_CHECK(cudaEventSynchronize(hp.slot_ev[size_t(kSlots) + j % kSlots]));
-          hp.pool->copy(v_host + out[j].first, hp.ring_out.get() + int64_t(j % kSlots) * kSlotElems,
+          copy_pool().copy(v_host + out[j].first, hp.ring_out.get() + int64_t(j % kSlots) * kSlotElems,
                         size_t(out[j].count) * sizeof(double));
         }
       } catch (const std::exception& e) {
@@ -316,7 +328,7 @@ void mass_apply_host_pipelined(MassPlan& p, const double* u_host, double* v_host
       cudaEvent_t e = hp.slot_ev[size_t(slot)];
       FEM_CUDA_CHECK(cudaEventSynchronize(e));  // the slot's previous copy is done (never recorded: at once)
       double* st = hp.ring_in.get() + int64_t(slot) * kSlotElems;
-      hp.pool->copy(st, u_host + first + off, size_t(n) * sizeof(double));
+      copy_pool().copy(st, u_host + first + off, size_t(n) * sizeof(double));
       FEM_CUDA_CHECK(cudaMemcpyAsync(hu + first + off, st, size_t(n) * sizeof(double), cudaMemcpyHostToDevice,
                                      hp.h2d));
       FEM_CUDA_CHECK(cudaEventRecord(e, hp.h2d));

@@ -185,15 +185,14 @@ struct HostPipeline {
   int target = 0;               // the chunk count it was built for
   std::vector<int64_t> lo, hi;  // per chunk: smallest and largest offset of its elements
   // staging for pageable host vectors, made by the first such apply: a ring
-  // of page-locked slots per direction, an event per slot, a memcpy pool
+  // of page-locked slots per direction and an event per slot (the memcpy
+  // threads are one pool for the process, host_apply.cu)
   PinnedBuf<double> ring_in, ring_out;
   std::vector<cudaEvent_t> slot_ev;  // kSlots for the copies in, then kSlots for the copies out
-  std::unique_ptr<CopyPool> pool;
   HostPipeline() = default;
   HostPipeline(const HostPipeline&) = delete;
   HostPipeline& operator=(const HostPipeline&) = delete;
   ~HostPipeline() {
-    pool.reset();
     for (cudaEvent_t e : slot_ev)
       if (e) (void)cudaEventDestroy(e);
     for (cudaEvent_t e : ev)
