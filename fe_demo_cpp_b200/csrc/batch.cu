@@ -74,7 +74,8 @@ __device__ __forceinline__ void with_interp(const Mat1D<P, Q, T>& mp, F&& body) 
   }
 }
 
-template <int P, int Q, int MINB, class T, int NCB>
+// EO: the even-odd contractions (eo_fwd / eo_bwd; centro-symmetric B).
+template <int P, int Q, int MINB, class T, int NCB, bool EO = false>
 __global__ void __launch_bounds__(Mass3D<P, Q>::NT, MINB)
     mass3d_batch_kernel(const __grid_constant__ Mat1D<P, Q, T> m, const BatchMesh<T>* __restrict__ meshes,
                         const int2* __restrict__ tiles, int64_t n_tiles) {
@@ -87,8 +88,9 @@ __global__ void __launch_bounds__(Mass3D<P, Q>::NT, MINB)
     for (int64_t g = blockIdx.x; g < n_tiles; g += gridDim.x) {
       const int2 tm = tiles[g];
       const BatchMesh<T> mm = meshes[tm.x];
-      mass3d_tile<P, Q, T, ApplyPlain, NCB>(mat, sa, sb, mm.offs, mm.qd, mm.u, mm.v, nullptr, mm.num_elem,
-                                            mm.comp_run, mm.comp_stride, ApplyPlain{}, tm.y, dsum);
+      mass3d_tile<P, Q, T, ApplyPlain, NCB, T, std::decay_t<decltype(mat)>, EO>(
+          mat, sa, sb, mm.offs, mm.qd, mm.u, mm.v, nullptr, mm.num_elem, mm.comp_run, mm.comp_stride, ApplyPlain{},
+          tm.y, dsum);
     }
   });
 }
@@ -135,6 +137,7 @@ Mat1D<P, Q, T> batch_mat(const BasisData& b) {
   Mat1D<P, Q, T> m;
   for (int i = 0; i < Q * P; ++i) m.B[i] = T(b.interp[i]), m.G[i] = T(b.grad[i]);
   for (int i = 0; i < Q; ++i) m.W[i] = T(b.q_weight[i]);
+  fill_eo(m);
   return m;
 }
 
@@ -145,6 +148,7 @@ using ClassLauncher = unsigned (*)(const BatchClass&, const void* meshes, unsign
 
 struct BatchClass {
   int dim = 0, P = 0, Q = 0, comp_run = 0, ncb = 1;
+  bool centro_symmetric = false;  // the members' B (one per class): even-odd contractions apply
   BasisData basis;
   std::vector<int> members;  // indices into the batch
   DevBuf<int2> tiles;
@@ -168,12 +172,17 @@ constexpr int batch_min_blocks(int P, int threads, int ncb, bool shared_matrix =
   return P >= 8 ? 1 : 0;  // as the single-mesh kernel (plain_min_blocks)
 }
 
-template <int P, int Q, class T, int NCB>
+// FP64 classes at P = 4 and 6 use the even-odd contractions when their B is
+// centro-symmetric (as the single-mesh one-tile kernel, plain_even_odd).
+template <int P, int Q, class T, int NCB, bool EO = (P == 4 || P == 6) && sizeof(T) == 8 && NCB == 1>
 unsigned launch_batch3(const BatchClass& c, const void* meshes, unsigned grid, cudaStream_t s) {
+  if constexpr (EO) {
+    if (!c.centro_symmetric) return launch_batch3<P, Q, T, NCB, false>(c, meshes, grid, s);
+  }
   using L = Mass3D<P, Q>;
   constexpr int smem = NCB * (L::SA + L::SB) * int(sizeof(T));
   constexpr int minb = batch_min_blocks(P, L::NT, NCB, batch_shared_matrix<P, T>());
-  const auto kern = mass3d_batch_kernel<P, Q, minb, T, NCB>;
+  const auto kern = mass3d_batch_kernel<P, Q, minb, T, NCB, EO>;
   static std::atomic<uint64_t> smem_set{0};
   set_smem(kern, smem, smem_set);
   if (grid == 0) grid = unsigned(std::min<int64_t>(resident_ctas(reinterpret_cast<const void*>(kern), L::NT, smem),
@@ -416,6 +425,7 @@ int fem_b200_batch_create(const fem_b200_mass* ops, int num_ops, int precision, 
         BatchClass c;
         c.dim = p.dim, c.P = p.P, c.Q = p.Q, c.comp_run = p.comp_run;
         c.basis = p.basis;
+        c.centro_symmetric = p.centro_symmetric;
         // three components through each phase together in FP32 only: for FP64
         // classes one at a time measured faster (512 uneven meshes, one graph:
         // 58.0 -> 62.1 GDoF/s), as for the FP64 Krylov apply

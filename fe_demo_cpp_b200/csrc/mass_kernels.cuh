@@ -47,7 +47,80 @@ struct Mat1D {
   T B[Q * P];  // interp_1d, row-major [q][p]
   T G[Q * P];  // grad_1d (the diagonal kernels carry interp_1d squared here)
   T W[Q];      // q_weight_1d
+  // Even-odd folds of B for the even-odd contractions (eo_fwd / eo_bwd),
+  // filled by fill_eo: for q < ceil(Q/2), j < P/2,
+  //   Ep[q][j] = (B[q][j] + B[q][P-1-j]) / 2,  Em[q][j] = (B[q][j] - B[q][P-1-j]) / 2.
+  T Ep[((Q + 1) / 2) * (P / 2)];
+  T Em[(Q / 2) * (P / 2)];
 };
+
+// Fills Mat1D::Ep / Em from B (host).
+template <int P, int Q, class T>
+void fill_eo(Mat1D<P, Q, T>& m) {
+  constexpr int HP = P / 2;
+  for (int q = 0; q < (Q + 1) / 2; ++q)
+    for (int j = 0; j < HP; ++j) m.Ep[q * HP + j] = (m.B[q * P + j] + m.B[q * P + P - 1 - j]) / 2;
+  for (int q = 0; q < Q / 2; ++q)
+    for (int j = 0; j < HP; ++j) m.Em[q * HP + j] = (m.B[q * P + j] - m.B[q * P + P - 1 - j]) / 2;
+}
+
+// Even-odd forms of the 1D contractions, for a centro-symmetric B
+// (B[Q-1-q][P-1-p] = B[q][p]: Lagrange bases on symmetric nodes evaluated at
+// symmetric points, e.g. GLL nodes and Gauss points).  With xe = x[j] +
+// x[P-1-j], xo = x[j] - x[P-1-j], the outputs q and Q-1-q are E + O and E - O
+// with E = sum Ep xe (+ the middle column for odd P) and O = sum Em xo: about
+// 17% fewer multiply-adds at P = 5, Q = 6, and dependency chains of P/2
+// instead of P.  The sums are regrouped, so results agree with the direct
+// contraction to rounding, not bitwise.
+// out[q] = sum_p B[q][p] x[p]
+template <int P, int Q, class T, class M>
+__device__ __forceinline__ void eo_fwd(const M& m, const T (&x)[P], T (&out)[Q]) {
+  constexpr int HP = P / 2, HQ = Q / 2;
+  T xe[HP], xo[HP];
+#pragma unroll
+  for (int j = 0; j < HP; ++j) xe[j] = x[j] + x[P - 1 - j], xo[j] = x[j] - x[P - 1 - j];
+#pragma unroll
+  for (int q = 0; q < (Q + 1) / 2; ++q) {
+    T e = (P & 1) ? m.B[q * P + HP] * x[HP] : T(0);
+#pragma unroll
+    for (int j = 0; j < HP; ++j) e += m.Ep[q * HP + j] * xe[j];
+    if (q < HQ) {
+      T o = T(0);
+#pragma unroll
+      for (int j = 0; j < HP; ++j) o += m.Em[q * HP + j] * xo[j];
+      out[q] = e + o;
+      out[Q - 1 - q] = e - o;
+    } else {
+      out[q] = e;  // the middle point of an odd Q: its odd part vanishes
+    }
+  }
+}
+
+// out[p] = sum_q B[q][p] y[q]
+template <int P, int Q, class T, class M>
+__device__ __forceinline__ void eo_bwd(const M& m, const T (&y)[Q], T (&out)[P]) {
+  constexpr int HP = P / 2, HQ = Q / 2;
+  T ye[HQ], yo[HQ];
+#pragma unroll
+  for (int i = 0; i < HQ; ++i) ye[i] = y[i] + y[Q - 1 - i], yo[i] = y[i] - y[Q - 1 - i];
+#pragma unroll
+  for (int p = 0; p < HP; ++p) {
+    T e = (Q & 1) ? m.B[HQ * P + p] * y[HQ] : T(0);
+#pragma unroll
+    for (int i = 0; i < HQ; ++i) e += m.Ep[i * HP + p] * ye[i];
+    T o = T(0);
+#pragma unroll
+    for (int i = 0; i < HQ; ++i) o += m.Em[i * HP + p] * yo[i];
+    out[p] = e + o;
+    out[P - 1 - p] = e - o;
+  }
+  if constexpr (P & 1) {  // the middle node of an odd P: its odd part vanishes
+    T e = (Q & 1) ? m.B[HQ * P + HP] * y[HQ] : T(0);
+#pragma unroll
+    for (int i = 0; i < HQ; ++i) e += m.B[i * P + HP] * ye[i];
+    out[HP] = e;
+  }
+}
 
 // The interpolation matrix read from a shared-memory copy at every use (the
 // volatile read keeps the compiler from holding all P*Q entries in registers
@@ -143,7 +216,7 @@ __device__ __forceinline__ void prefetch_tile_l2(const int* offs, const S* qd, i
 
 // One 8-element tile of the 3D fused apply (the body of mass3d_apply_kernel and
 // of the batched kernels): sa / sb are the CTA's shared buffers A and B.
-template <int P, int Q, class T, class Ext, int NCB, class S = T, class M = Mat1D<P, Q, T>>
+template <int P, int Q, class T, class Ext, int NCB, class S = T, class M = Mat1D<P, Q, T>, bool EO = false>
 __device__ __forceinline__ void mass3d_tile(const M& m, T* __restrict__ sa, T* __restrict__ sb,
                                             const int* __restrict__ offs, const S* __restrict__ qd,
                                             const S* __restrict__ u, T* __restrict__ v, T* __restrict__ ev,
@@ -187,12 +260,19 @@ __device__ __forceinline__ void mass3d_tile(const M& m, T* __restrict__ sa, T* _
       const int px = col % P, py = col / P;
 #pragma unroll
       for (int c = 0; c < NCB; ++c) {
+        if constexpr (EO) {
+          T o[Q];
+          eo_fwd<P, Q>(m, x[c], o);
 #pragma unroll
-        for (int qz = 0; qz < Q; ++qz) {
-          T s = T(0);
+          for (int qz = 0; qz < Q; ++qz) sa[c * L::SA + py * L::PS1 + (qz * P + px) * E + e] = o[qz];
+        } else {
 #pragma unroll
-          for (int pz = 0; pz < P; ++pz) s += m.B[qz * P + pz] * x[c][pz];
-          sa[c * L::SA + py * L::PS1 + (qz * P + px) * E + e] = s;
+          for (int qz = 0; qz < Q; ++qz) {
+            T s = T(0);
+#pragma unroll
+            for (int pz = 0; pz < P; ++pz) s += m.B[qz * P + pz] * x[c][pz];
+            sa[c * L::SA + py * L::PS1 + (qz * P + px) * E + e] = s;
+          }
         }
       }
     }
@@ -204,12 +284,19 @@ __device__ __forceinline__ void mass3d_tile(const M& m, T* __restrict__ sa, T* _
         T y[P];
 #pragma unroll
         for (int py = 0; py < P; ++py) y[py] = sa[c * L::SA + py * L::PS1 + col * E + e];
+        if constexpr (EO) {
+          T o[Q];
+          eo_fwd<P, Q>(m, y, o);
 #pragma unroll
-        for (int qy = 0; qy < Q; ++qy) {
-          T s = T(0);
+          for (int qy = 0; qy < Q; ++qy) sb[c * L::SB + px * L::PS2 + (qz * Q + qy) * E + e] = o[qy];
+        } else {
 #pragma unroll
-          for (int py = 0; py < P; ++py) s += m.B[qy * P + py] * y[py];
-          sb[c * L::SB + px * L::PS2 + (qz * Q + qy) * E + e] = s;
+          for (int qy = 0; qy < Q; ++qy) {
+            T s = T(0);
+#pragma unroll
+            for (int py = 0; py < P; ++py) s += m.B[qy * P + py] * y[py];
+            sb[c * L::SB + px * L::PS2 + (qz * Q + qy) * E + e] = s;
+          }
         }
       }
     }
@@ -222,20 +309,34 @@ __device__ __forceinline__ void mass3d_tile(const M& m, T* __restrict__ sa, T* _
 #pragma unroll
         for (int px = 0; px < P; ++px) w[px] = sb[c * L::SB + px * L::PS2 + col * E + e];
         T r[Q];
+        if constexpr (EO) {
+          T t[Q];
+          eo_fwd<P, Q>(m, w, t);
 #pragma unroll
-        for (int qx = 0; qx < Q; ++qx) {
-          T s = T(0);
+          for (int qx = 0; qx < Q; ++qx) {
+            r[qx] = qv[qx] * t[qx];
+            if constexpr (Ext::kDot) dsum += double(r[qx]) * double(t[qx]);
+          }
+          T o[P];
+          eo_bwd<P, Q>(m, r, o);
 #pragma unroll
-          for (int px = 0; px < P; ++px) s += m.B[qx * P + px] * w[px];
-          r[qx] = qv[qx] * s;
-          if constexpr (Ext::kDot) dsum += double(r[qx]) * double(s);
-        }
+          for (int px = 0; px < P; ++px) sa[c * L::SA + qy * L::PS3 + (qz * P + px) * E + e] = o[px];
+        } else {
 #pragma unroll
-        for (int px = 0; px < P; ++px) {
-          T s = T(0);
+          for (int qx = 0; qx < Q; ++qx) {
+            T s = T(0);
 #pragma unroll
-          for (int qx = 0; qx < Q; ++qx) s += m.B[qx * P + px] * r[qx];
-          sa[c * L::SA + qy * L::PS3 + (qz * P + px) * E + e] = s;
+            for (int px = 0; px < P; ++px) s += m.B[qx * P + px] * w[px];
+            r[qx] = qv[qx] * s;
+            if constexpr (Ext::kDot) dsum += double(r[qx]) * double(s);
+          }
+#pragma unroll
+          for (int px = 0; px < P; ++px) {
+            T s = T(0);
+#pragma unroll
+            for (int qx = 0; qx < Q; ++qx) s += m.B[qx * P + px] * r[qx];
+            sa[c * L::SA + qy * L::PS3 + (qz * P + px) * E + e] = s;
+          }
         }
       }
     }
@@ -247,12 +348,19 @@ __device__ __forceinline__ void mass3d_tile(const M& m, T* __restrict__ sa, T* _
         T y[Q];
 #pragma unroll
         for (int qy = 0; qy < Q; ++qy) y[qy] = sa[c * L::SA + qy * L::PS3 + col * E + e];
+        if constexpr (EO) {
+          T o[P];
+          eo_bwd<P, Q>(m, y, o);
 #pragma unroll
-        for (int py = 0; py < P; ++py) {
-          T s = T(0);
+          for (int py = 0; py < P; ++py) sb[c * L::SB + qz * L::PS4 + (py * P + px) * E + e] = o[py];
+        } else {
 #pragma unroll
-          for (int qy = 0; qy < Q; ++qy) s += m.B[qy * P + py] * y[qy];
-          sb[c * L::SB + qz * L::PS4 + (py * P + px) * E + e] = s;
+          for (int py = 0; py < P; ++py) {
+            T s = T(0);
+#pragma unroll
+            for (int qy = 0; qy < Q; ++qy) s += m.B[qy * P + py] * y[qy];
+            sb[c * L::SB + qz * L::PS4 + (py * P + px) * E + e] = s;
+          }
         }
       }
     }
@@ -264,11 +372,17 @@ __device__ __forceinline__ void mass3d_tile(const M& m, T* __restrict__ sa, T* _
 #pragma unroll
         for (int qz = 0; qz < Q; ++qz) z[qz] = sb[c * L::SB + qz * L::PS4 + col * E + e];
         const int64_t ks = (k0 + c) * comp_stride;
+        T zo[P];
+        if constexpr (EO) eo_bwd<P, Q>(m, z, zo);
 #pragma unroll
         for (int pz = 0; pz < P; ++pz) {
           T s = T(0);
+          if constexpr (EO) {
+            s = zo[pz];
+          } else {
 #pragma unroll
-          for (int qz = 0; qz < Q; ++qz) s += m.B[qz * P + pz] * z[qz];
+            for (int qz = 0; qz < Q; ++qz) s += m.B[qz * P + pz] * z[qz];
+          }
           if (valid) {
             if (ev)
               ev[(int64_t(k0 + c) * L::ES + pz * P * P + col) * num_elem + eg] = s;
@@ -305,7 +419,7 @@ __device__ __forceinline__ void mass3d_tile(const M& m, T* __restrict__ sa, T* _
 // there instead of waiting on DRAM (P = 5: 1.05x sustained); persistent (Ext
 // with a reduction), l2_ahead != 0: each CTA prefetches its next tile.
 template <int P, int Q, int MINB = 1, class T = double, class Ext = ApplyPlain, int NCB = 1, class S = T,
-          bool SB = false>
+          bool SB = false, bool EO = false>
 __global__ void __launch_bounds__(Mass3D<P, Q>::NT, MINB) mass3d_apply_kernel(
     const __grid_constant__ Mat1D<P, Q, T> m, const int* __restrict__ offs, const S* __restrict__ qd,
     const S* __restrict__ u, T* __restrict__ v, T* __restrict__ ev, int num_elem, int num_comp_run,
@@ -331,14 +445,15 @@ __global__ void __launch_bounds__(Mass3D<P, Q>::NT, MINB) mass3d_apply_kernel(
         // l2_ahead != 0: this CTA's next tile (a wave ahead) into L2 first
         if (l2_ahead != 0 && threadIdx.x == 0 && tile + gridDim.x < n_tiles)
           prefetch_tile_l2<L::ES, L::NQ, E, S>(offs, qd, tile + gridDim.x);
-        mass3d_tile<P, Q, T, Ext, NCB, S>(mat, sa, sb, offs, qd, u, v, ev, num_elem, num_comp_run, comp_stride, ext,
-                                          tile, dsum);
+        mass3d_tile<P, Q, T, Ext, NCB, S, std::decay_t<decltype(mat)>, EO>(mat, sa, sb, offs, qd, u, v, ev, num_elem,
+                                                                           num_comp_run, comp_stride, ext, tile, dsum);
       }
       double dv[1] = {dsum};
       grid_sum<1>(dv, ext.part, &ext.st->ticket, [&](const double* tot) { cg_after_apply(ext.st, tot[0]); });
     } else {
-      mass3d_tile<P, Q, T, Ext, NCB, S>(mat, sa, sb, offs, qd, u, v, ev, num_elem, num_comp_run, comp_stride, ext,
-                                        blockIdx.x, dsum);
+      mass3d_tile<P, Q, T, Ext, NCB, S, std::decay_t<decltype(mat)>, EO>(mat, sa, sb, offs, qd, u, v, ev, num_elem,
+                                                                         num_comp_run, comp_stride, ext, blockIdx.x,
+                                                                         dsum);
     }
   };
   if constexpr (SB) {

@@ -213,6 +213,9 @@ struct MassPlan {
   int64_t comp_stride = 0;
   int tile_e = 0;
   int64_t n_tiles = 0;
+  // B[Q-1-q][P-1-p] = B[q][p] to rounding (symmetric nodes and points): the
+  // even-odd contractions (eo_fwd / eo_bwd) apply
+  bool centro_symmetric = false;
   BasisData basis;
   std::shared_ptr<RestrictionData> r;
   DevBuf<int> offs_t;
@@ -259,6 +262,7 @@ Mat1D<P, Q> make_mat(const BasisData& b) {
   std::memcpy(m.B, b.interp.data(), sizeof(m.B));
   std::memcpy(m.G, b.grad.data(), sizeof(m.G));
   std::memcpy(m.W, b.q_weight.data(), sizeof(m.W));
+  fill_eo(m);
   return m;
 }
 

@@ -198,8 +198,10 @@ def test_tail_tiles_and_single_element(fem, cuda, orc):
 @pytest.mark.parametrize("P,Q", [(2, 3), (3, 4), (4, 5), (5, 6), (6, 7), (8, 9)])
 def test_pipelined_equals_simple_on_many_tiles(fem, cuda, P, Q):
     """Several tiles per persistent CTA (a mesh larger than one wave), the
-    deterministic mode so every variant's output compares bitwise with the
-    one-tile kernel's (the variants the shape has)."""
+    deterministic mode so that variants contracting in the same order compare
+    bitwise (the variants the shape has).  At P = 4 and 6 the one-tile kernel
+    uses the even-odd contractions (regrouped sums): it is compared normwise
+    at 1e-14 with the others, which stay bitwise equal among themselves."""
     import torch
     m = box_mesh((40, 30, 20), P, seed=8)
     qd = build_qdata(fem, cuda, m, Q)
@@ -217,8 +219,13 @@ def test_pipelined_equals_simple_on_many_tiles(fem, cuda, P, Q):
         op.check()
         out[variant] = host(v)
     assert len(out) >= 5
+    even_odd = P in (4, 6)
+    ref = out[2] if (even_odd and 2 in out) else out[1]
     for variant, got in out.items():
-        assert np.array_equal(out[1], got), variant
+        if variant == 1 and even_odd:
+            close(got, ref, 1e-14)
+        else:
+            assert np.array_equal(ref, got), variant
 
 
 def test_autotune_picks_a_variant_and_keeps_parity(fem, cuda, orc):
