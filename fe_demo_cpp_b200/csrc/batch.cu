@@ -74,8 +74,9 @@ __device__ __forceinline__ void with_interp(const Mat1D<P, Q, T>& mp, F&& body) 
   }
 }
 
-// EO: the even-odd contractions (eo_fwd / eo_bwd; centro-symmetric B).
-template <int P, int Q, int MINB, class T, int NCB, bool EO = false>
+// EO: the even-odd contractions (eo_fwd / eo_bwd; centro-symmetric B); SB:
+// the 1D matrix from a shared copy (the high-order fallback without EO).
+template <int P, int Q, int MINB, class T, int NCB, bool EO = false, bool SB = batch_shared_matrix<P, T>() && !EO>
 __global__ void __launch_bounds__(Mass3D<P, Q>::NT, MINB)
     mass3d_batch_kernel(const __grid_constant__ Mat1D<P, Q, T> m, const BatchMesh<T>* __restrict__ meshes,
                         const int2* __restrict__ tiles, int64_t n_tiles) {
@@ -84,7 +85,7 @@ __global__ void __launch_bounds__(Mass3D<P, Q>::NT, MINB)
   T* sa = reinterpret_cast<T*>(smem_bytes);
   T* sb = sa + NCB * L::SA;
   double dsum = 0.0;
-  with_interp<batch_shared_matrix<P, T>()>(m, [&](const auto& mat) {
+  with_interp<SB>(m, [&](const auto& mat) {
     for (int64_t g = blockIdx.x; g < n_tiles; g += gridDim.x) {
       const int2 tm = tiles[g];
       const BatchMesh<T> mm = meshes[tm.x];
@@ -172,17 +173,20 @@ constexpr int batch_min_blocks(int P, int threads, int ncb, bool shared_matrix =
   return P >= 8 ? 1 : 0;  // as the single-mesh kernel (plain_min_blocks)
 }
 
-// FP64 classes at P = 4 and 6 use the even-odd contractions when their B is
-// centro-symmetric (as the single-mesh one-tile kernel, plain_even_odd).
-template <int P, int Q, class T, int NCB, bool EO = (P == 4 || P == 6) && sizeof(T) == 8 && NCB == 1>
+// FP64 classes at P = 4 and P >= 6 use the even-odd contractions when their
+// B is centro-symmetric (as the single-mesh one-tile kernel, plain_even_odd;
+// P = 7 with two resident CTAs); otherwise the direct form, from a shared
+// copy of the matrix at P >= 7.
+template <int P, int Q, class T, int NCB, bool EO = (P == 4 || P >= 6) && sizeof(T) == 8 && NCB == 1>
 unsigned launch_batch3(const BatchClass& c, const void* meshes, unsigned grid, cudaStream_t s) {
   if constexpr (EO) {
     if (!c.centro_symmetric) return launch_batch3<P, Q, T, NCB, false>(c, meshes, grid, s);
   }
   using L = Mass3D<P, Q>;
   constexpr int smem = NCB * (L::SA + L::SB) * int(sizeof(T));
-  constexpr int minb = batch_min_blocks(P, L::NT, NCB, batch_shared_matrix<P, T>());
-  const auto kern = mass3d_batch_kernel<P, Q, minb, T, NCB, EO>;
+  constexpr bool sb = batch_shared_matrix<P, T>() && !EO;
+  constexpr int minb = batch_min_blocks(P, L::NT, NCB, sb || (EO && P == 7));
+  const auto kern = mass3d_batch_kernel<P, Q, minb, T, NCB, EO, sb>;
   static std::atomic<uint64_t> smem_set{0};
   set_smem(kern, smem, smem_set);
   if (grid == 0) grid = unsigned(std::min<int64_t>(resident_ctas(reinterpret_cast<const void*>(kern), L::NT, smem),

@@ -60,19 +60,31 @@ constexpr bool plain_shared_matrix() {
 // P = 6 1.06x; sustained (300 launches, interleaved with the kernel without
 // it) P = 5 1.05x.
 // The even-odd contractions (eo_fwd / eo_bwd) where they measured faster, for
-// a centro-symmetric B: P = 6 1.53x (68 registers without spills instead of
-// 72 with 84 B), P = 4 1.08x; P = 5 equal, so it keeps the direct form.
+// a centro-symmetric B: P = 4 1.10x, P = 6 1.53x (68 registers without spills
+// instead of 72 with 84 B), P = 7 1.85x and P = 8 1.47x against the
+// shared-matrix form (the folds are half of B, so holding them in registers
+// no longer starves the CTA: P = 7 two CTAs at 64 registers, no spills); P = 5
+// equal, so it keeps the direct form.
 template <int P>
 constexpr bool plain_even_odd() {
-  return P == 4 || P == 6;
+  return P == 4 || P >= 6;
 }
 
-template <int P, int Q, int MINB = plain_min_blocks<P>(), bool SB = plain_shared_matrix<P>() && MINB == plain_min_blocks<P>(),
-          bool EO = plain_even_odd<P>() && !SB && MINB == plain_min_blocks<P>()>
+template <int P, int Q, int MINB, bool SB, bool EO>
+void launch_apply3_kernel(const MassPlan& p, const double* u, double* v, double* ev, cudaStream_t s);
+
+// The simple variant: even-odd where it applies, else the direct form
+// (shared-memory matrix at P >= 7).
+template <int P, int Q>
 void launch_apply3(const MassPlan& p, const double* u, double* v, double* ev, cudaStream_t s) {
-  if constexpr (EO) {
-    if (!p.centro_symmetric) return launch_apply3<P, Q, MINB, SB, false>(p, u, v, ev, s);
+  if constexpr (plain_even_odd<P>()) {
+    if (p.centro_symmetric) return launch_apply3_kernel<P, Q, plain_min_blocks<P>(), false, true>(p, u, v, ev, s);
   }
+  launch_apply3_kernel<P, Q, plain_min_blocks<P>(), plain_shared_matrix<P>(), false>(p, u, v, ev, s);
+}
+
+template <int P, int Q, int MINB, bool SB, bool EO>
+void launch_apply3_kernel(const MassPlan& p, const double* u, double* v, double* ev, cudaStream_t s) {
   using L = Mass3D<P, Q>;
   const auto kern = mass3d_apply_kernel<P, Q, MINB, double, ApplyPlain, 1, double, SB, EO>;
   static std::atomic<uint64_t> smem_set{0};
@@ -222,7 +234,7 @@ struct Table {
     if constexpr (Pipe3D<P, Q>::SMEM <= kMaxSmemPerCta) pp[P][DQ] = launch_apply3_pipe<P, Q>;
     if constexpr (Mass3DX2<P, Q>::SMEM <= kMaxSmemPerCta && Mass3DX2<P, Q>::NT <= 1024) xx[P][DQ] = launch_apply3_x2<P, Q>;
     if constexpr (Prefetch3D<P, Q>::SMEM <= kMaxSmemPerCta) pf[P][DQ] = launch_apply3_pf<P, Q>;
-    if constexpr (Mass3D<P, Q>::MINB_OCC > 1) oc[P][DQ] = launch_apply3<P, Q, Mass3D<P, Q>::MINB_OCC>;
+    if constexpr (Mass3D<P, Q>::MINB_OCC > 1) oc[P][DQ] = launch_apply3_kernel<P, Q, Mass3D<P, Q>::MINB_OCC, false, false>;
     if constexpr (Narrow3D<P, Q>::SMEM <= kMaxSmemPerCta) nw[P][DQ] = launch_apply3_narrow<P, Q>;
     if constexpr (P <= 3) el[P][DQ] = launch_apply3_element<P, Q>;  // registers: 86 (P=2), 250 (P=3)
     bd[0][P][DQ] = launch_build1<P, Q>;
@@ -291,14 +303,12 @@ ApplyLauncher variant_launcher(const MassPlan& p, int variant) {
 // The variant a plan runs until it is autotuned: where one variant beat the
 // one-tile kernel on every B200 of the order sweep (64M-DoF box meshes,
 // Q = P + 1, one and three components), that one; else the one-tile kernel.
-// element at P <= 3 (P = 2: 2.5x, P = 3: 1.1-1.15x), prefetch at P = 7
-// (level with the shared-matrix one-tile kernel for one component, 1.1x for
-// three).  Other orders and quadratures: their best variant moves from box to
-// box, which the autotuner settles.
+// element at P <= 3 (P = 2: 2.5x, P = 3: 1.1-1.15x).  Elsewhere the one-tile
+// kernel (with the even-odd contractions at P = 4 and P >= 6 it leads at
+// every order from 4 to 8; the ranking of the others moves from box to box,
+// which the autotuner settles).
 int default_variant(const MassPlan& p) {
-  if (p.dim != 3 || p.Q != p.P + 1) return FEM_B200_KERNEL_SIMPLE;
-  if (p.P <= 3) return FEM_B200_KERNEL_ELEMENT;
-  if (p.P == 7) return FEM_B200_KERNEL_PREFETCH;
+  if (p.dim == 3 && p.Q == p.P + 1 && p.P <= 3) return FEM_B200_KERNEL_ELEMENT;
   return FEM_B200_KERNEL_SIMPLE;
 }
 

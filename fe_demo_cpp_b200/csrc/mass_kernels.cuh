@@ -129,6 +129,8 @@ __device__ __forceinline__ void eo_bwd(const M& m, const T (&y)[Q], T (&out)[P])
 template <class T>
 struct SharedB {
   const volatile T* B;
+  const volatile T* Ep = nullptr;  // shared copies of Mat1D::Ep / Em (the even-odd contractions)
+  const volatile T* Em = nullptr;
 };
 
 // Shared-memory plane stride for a tile of 8 elements: an odd multiple of 8
@@ -457,10 +459,18 @@ __global__ void __launch_bounds__(Mass3D<P, Q>::NT, MINB) mass3d_apply_kernel(
     }
   };
   if constexpr (SB) {
-    __shared__ T b_s[P * Q];
+    constexpr int NP = ((Q + 1) / 2) * (P / 2), NM = (Q / 2) * (P / 2);
+    __shared__ T b_s[P * Q + (EO ? NP + NM : 0)];
     for (int i = threadIdx.x; i < P * Q; i += blockDim.x) b_s[i] = m.B[i];
+    if constexpr (EO) {
+      for (int i = threadIdx.x; i < NP; i += blockDim.x) b_s[P * Q + i] = m.Ep[i];
+      for (int i = threadIdx.x; i < NM; i += blockDim.x) b_s[P * Q + NP + i] = m.Em[i];
+    }
     __syncthreads();
-    run(SharedB<T>{b_s});
+    if constexpr (EO)
+      run(SharedB<T>{b_s, b_s + P * Q, b_s + P * Q + NP});
+    else
+      run(SharedB<T>{b_s});
   } else {
     run(m);
   }

@@ -310,6 +310,7 @@ Mat1D<P, Q, T> typed_mat(const BasisData& b) {
   Mat1D<P, Q, T> m;
   for (int i = 0; i < Q * P; ++i) m.B[i] = T(b.interp[i]), m.G[i] = T(b.grad[i]);
   for (int i = 0; i < Q; ++i) m.W[i] = T(b.q_weight[i]);
+  fill_eo(m);
   return m;
 }
 
@@ -352,17 +353,23 @@ unsigned resident_grid(K kernel, int threads, int smem, int64_t n_tiles) {
 
 // w (+)= M (dinv . r) with delta = (dinv . r)^T M (dinv . r) reduced into the
 // solver scalars.  ev != nullptr: element contributions to the E-vector.
-template <int P, int Q, class T, int NCB>
+template <int P, int Q, class T, int NCB, bool EO = (P == 4 || P >= 6) && sizeof(T) == 8 && NCB == 1>
 void launch_cg_apply3(const MassPlan& p, const T* r, T* w, T* ev, const T* qd, const ApplyCg<T>& ext,
                       cudaStream_t s) {
   using L = Mass3D<P, Q>;
   constexpr int smem = NCB * (L::SA + L::SB) * int(sizeof(T));
   static std::atomic<uint64_t> smem_set{0};
-  // FP64 at P >= 7: the 1D matrix from a shared copy, as the one-tile apply.
-  // Last argument: each CTA prefetches its next tile into L2 (FP64 solve
-  // 57.2 -> 56.5 ms at 64^3, P = 5, 3 components; FP32 unchanged).
-  constexpr bool sb = P >= 7 && sizeof(T) == 8;
-  const auto kern = mass3d_apply_kernel<P, Q, cg_min_blocks(L::NT, P, sb), T, ApplyCg<T>, NCB, T, sb>;
+  // FP64, one component at a time: the even-odd contractions at P = 4 and
+  // P >= 6 for a centro-symmetric B (as the one-tile apply), else at P >= 7
+  // the direct form from a shared copy of the matrix.  Last argument: each CTA
+  // prefetches its next tile into L2 (FP64 solve 57.2 -> 56.5 ms at 64^3,
+  // P = 5, 3 components; FP32 unchanged).
+  if constexpr (EO) {
+    if (!p.centro_symmetric) return launch_cg_apply3<P, Q, T, NCB, false>(p, r, w, ev, qd, ext, s);
+  }
+  constexpr bool sb = P >= 7 && sizeof(T) == 8 && !EO;
+  const auto kern = mass3d_apply_kernel<P, Q, cg_min_blocks(L::NT, P, sb || (EO && P == 7)), T, ApplyCg<T>, NCB, T,
+                                        sb, EO>;
   set_smem(kern, smem, smem_set);
   kern<<<resident_grid(kern, L::NT, smem, p.n_tiles), L::NT, smem, s>>>(
       typed_mat<P, Q, T>(p.basis), p.offs_t.get(), qd, r, w, ev, p.num_elem, p.comp_run, p.comp_stride, ext, 1);

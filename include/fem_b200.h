@@ -58,7 +58,7 @@ extern "C" {
 #define FEM_B200_QF_APPLY_MASS 0        /* include/qfunctions/mass.hpp:45-51: component 0 only */
 #define FEM_B200_QF_APPLY_MASS_VECTOR 1 /* every component: v_k = qdata * u_k (no reference counterpart) */
 /* Kernel variants of the fused 3D mass apply (fem_b200_mass_set_kernel) */
-#define FEM_B200_KERNEL_AUTO 0      /* the autotuned variant for the shape (fem_b200_mass_autotune), else a measured per-order default (3D, Q = P+1: ELEMENT at P <= 3, PREFETCH at 7; SIMPLE otherwise) */
+#define FEM_B200_KERNEL_AUTO 0      /* the autotuned variant for the shape (fem_b200_mass_autotune), else a measured per-order default (3D, Q = P+1: ELEMENT at P <= 3; SIMPLE otherwise) */
 #define FEM_B200_KERNEL_SIMPLE 1    /* one CTA per 8-element tile, one element per thread */
 #define FEM_B200_KERNEL_PIPELINED 2 /* persistent CTAs, next tile staged by bulk copies during this one */
 #define FEM_B200_KERNEL_PAIRED 3    /* one CTA per 16 elements, two adjacent elements per thread */
