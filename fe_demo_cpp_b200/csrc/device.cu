@@ -168,11 +168,12 @@ void launch_apply3_element(const MassPlan& p, const double* u, double* v, double
 
 // dim 2: the interpolation matrix from shared memory at P >= 7, where holding
 // it in registers leaves one resident CTA (145-168 registers): 1.46x at
-// P = 7, 1.15x at P = 8 (16M-node boxes); slower below.
-template <int P, int Q>
-void launch_apply2(const MassPlan& p, const double* u, double* v, double* ev, cudaStream_t s) {
+// P = 7, 1.15x at P = 8 (16M-node boxes); slower below.  EO: the even-odd
+// contractions (centro-symmetric B), in place of it.
+template <int P, int Q, bool SB, bool EO>
+void launch_apply2_kernel(const MassPlan& p, const double* u, double* v, double* ev, cudaStream_t s) {
   using L = Mass2D<P, Q>;
-  const auto kern = mass2d_apply_kernel<P, Q, double, ApplyPlain, double, 0, (P >= 7)>;
+  const auto kern = mass2d_apply_kernel<P, Q, double, ApplyPlain, double, 0, SB, EO>;
   static std::atomic<uint64_t> smem_set{0};
   set_smem(kern, L::SMEM, smem_set);
   // L2 prefetch a wave ahead at P <= 4 (P = 2, 3: 1.10-1.12x one component,
@@ -181,6 +182,22 @@ void launch_apply2(const MassPlan& p, const double* u, double* v, double* ev, cu
   kern<<<unsigned(p.tiles()), L::NT, L::SMEM, s>>>(make_mat<P, Q>(p.basis), p.offs(), p.qd(), u, v, ev, p.elems(),
                                                    p.comp_run, p.comp_stride, ApplyPlain{}, wave);
   FEM_LAUNCH_CHECK();
+}
+
+// dim 2 even-odd where it measured faster (interleaved A/B, ~64M-DoF quad
+// boxes): P = 6 1.52x, P = 7 1.82x, P = 8 1.51x (three components 1.32-1.76x);
+// P = 4, 5 equal.
+template <int P>
+constexpr bool plain_even_odd_2d() {
+  return P >= 6;
+}
+
+template <int P, int Q>
+void launch_apply2(const MassPlan& p, const double* u, double* v, double* ev, cudaStream_t s) {
+  if constexpr (plain_even_odd_2d<P>()) {
+    if (p.centro_symmetric) return launch_apply2_kernel<P, Q, false, true>(p, u, v, ev, s);
+  }
+  launch_apply2_kernel<P, Q, (P >= 7), false>(p, u, v, ev, s);
 }
 
 template <int P, int Q>

@@ -610,7 +610,7 @@ struct Mass2D {
 };
 
 // One 32-element tile of the 2D fused apply: s1 / s3 the CTA's shared buffers.
-template <int P, int Q, class T, class Ext, class S = T, class M = Mat1D<P, Q, T>>
+template <int P, int Q, class T, class Ext, class S = T, class M = Mat1D<P, Q, T>, bool EO = false>
 __device__ __forceinline__ void mass2d_tile(const M& m, T* __restrict__ s1, T* __restrict__ s3,
                                             const int* __restrict__ offs, const S* __restrict__ qd,
                                             const S* __restrict__ u, T* __restrict__ v, T* __restrict__ ev,
@@ -643,12 +643,19 @@ __device__ __forceinline__ void mass2d_tile(const M& m, T* __restrict__ s1, T* _
         x[py] = load_as<T>(u + off[py] + ks);
         if constexpr (Ext::kScale) x[py] *= __ldg(ext.scale + off[py]);
       }
+      if constexpr (EO) {
+        T o[Q];
+        eo_fwd<P, Q>(m, x, o);
 #pragma unroll
-      for (int qy = 0; qy < Q; ++qy) {
-        T s = T(0);
+        for (int qy = 0; qy < Q; ++qy) s1[(col * Q + qy) * E + e] = o[qy];
+      } else {
 #pragma unroll
-        for (int py = 0; py < P; ++py) s += m.B[qy * P + py] * x[py];
-        s1[(col * Q + qy) * E + e] = s;
+        for (int qy = 0; qy < Q; ++qy) {
+          T s = T(0);
+#pragma unroll
+          for (int py = 0; py < P; ++py) s += m.B[qy * P + py] * x[py];
+          s1[(col * Q + qy) * E + e] = s;
+        }
       }
     }
     __syncthreads();
@@ -657,20 +664,34 @@ __device__ __forceinline__ void mass2d_tile(const M& m, T* __restrict__ s1, T* _
 #pragma unroll
       for (int px = 0; px < P; ++px) w[px] = s1[(px * Q + col) * E + e];
       T r[Q];
+      if constexpr (EO) {
+        T t[Q];
+        eo_fwd<P, Q>(m, w, t);
 #pragma unroll
-      for (int qx = 0; qx < Q; ++qx) {
-        T s = T(0);
+        for (int qx = 0; qx < Q; ++qx) {
+          r[qx] = qv[qx] * t[qx];
+          if constexpr (Ext::kDot) dsum += double(r[qx]) * double(t[qx]);
+        }
+        T o[P];
+        eo_bwd<P, Q>(m, r, o);
 #pragma unroll
-        for (int px = 0; px < P; ++px) s += m.B[qx * P + px] * w[px];
-        r[qx] = qv[qx] * s;
-        if constexpr (Ext::kDot) dsum += double(r[qx]) * double(s);
-      }
+        for (int px = 0; px < P; ++px) s3[(col * P + px) * E + e] = o[px];
+      } else {
 #pragma unroll
-      for (int px = 0; px < P; ++px) {
-        T s = T(0);
+        for (int qx = 0; qx < Q; ++qx) {
+          T s = T(0);
 #pragma unroll
-        for (int qx = 0; qx < Q; ++qx) s += m.B[qx * P + px] * r[qx];
-        s3[(col * P + px) * E + e] = s;
+          for (int px = 0; px < P; ++px) s += m.B[qx * P + px] * w[px];
+          r[qx] = qv[qx] * s;
+          if constexpr (Ext::kDot) dsum += double(r[qx]) * double(s);
+        }
+#pragma unroll
+        for (int px = 0; px < P; ++px) {
+          T s = T(0);
+#pragma unroll
+          for (int qx = 0; qx < Q; ++qx) s += m.B[qx * P + px] * r[qx];
+          s3[(col * P + px) * E + e] = s;
+        }
       }
     }
     __syncthreads();
@@ -678,11 +699,17 @@ __device__ __forceinline__ void mass2d_tile(const M& m, T* __restrict__ s1, T* _
       T z[Q];
 #pragma unroll
       for (int qy = 0; qy < Q; ++qy) z[qy] = s3[(qy * P + col) * E + e];
+      T zo[P];
+      if constexpr (EO) eo_bwd<P, Q>(m, z, zo);
 #pragma unroll
       for (int py = 0; py < P; ++py) {
         T s = T(0);
+        if constexpr (EO) {
+          s = zo[py];
+        } else {
 #pragma unroll
-        for (int qy = 0; qy < Q; ++qy) s += m.B[qy * P + py] * z[qy];
+          for (int qy = 0; qy < Q; ++qy) s += m.B[qy * P + py] * z[qy];
+        }
         if (valid) {
           if (ev)
             ev[(int64_t(k) * L::ES + py * P + col) * num_elem + eg] = s;
@@ -699,7 +726,8 @@ __device__ __forceinline__ void mass2d_tile(const M& m, T* __restrict__ s1, T* _
 // copy (SharedB) instead of the kernel parameter.  l2_ahead > 0 (one CTA per
 // tile): CTA b has tile b + l2_ahead's qdata and offsets prefetched into L2,
 // as the 3D kernel.
-template <int P, int Q, class T = double, class Ext = ApplyPlain, class S = T, int MINB = 0, bool SB = false>
+template <int P, int Q, class T = double, class Ext = ApplyPlain, class S = T, int MINB = 0, bool SB = false,
+          bool EO = false>
 __global__ void __launch_bounds__(Mass2D<P, Q>::NT, MINB) mass2d_apply_kernel(
     const __grid_constant__ Mat1D<P, Q, T> m, const int* __restrict__ offs, const S* __restrict__ qd,
     const S* __restrict__ u, T* __restrict__ v, T* __restrict__ ev, int num_elem, int num_comp_run,
@@ -722,13 +750,13 @@ __global__ void __launch_bounds__(Mass2D<P, Q>::NT, MINB) mass2d_apply_kernel(
     if constexpr (Ext::kDot) {  // persistent, one reduction per CTA
       const int64_t n_tiles = (int64_t(num_elem) + E - 1) / E;
       for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x)
-        mass2d_tile<P, Q, T, Ext, S>(mat, s1, s3, offs, qd, u, v, ev, num_elem, num_comp_run, comp_stride, ext,
-                                     tile, dsum);
+        mass2d_tile<P, Q, T, Ext, S, std::decay_t<decltype(mat)>, EO>(mat, s1, s3, offs, qd, u, v, ev, num_elem,
+                                                                      num_comp_run, comp_stride, ext, tile, dsum);
       double dv[1] = {dsum};
       grid_sum<1>(dv, ext.part, &ext.st->ticket, [&](const double* tot) { cg_after_apply(ext.st, tot[0]); });
     } else {
-      mass2d_tile<P, Q, T, Ext, S>(mat, s1, s3, offs, qd, u, v, ev, num_elem, num_comp_run, comp_stride, ext,
-                                   blockIdx.x, dsum);
+      mass2d_tile<P, Q, T, Ext, S, std::decay_t<decltype(mat)>, EO>(mat, s1, s3, offs, qd, u, v, ev, num_elem,
+                                                                    num_comp_run, comp_stride, ext, blockIdx.x, dsum);
     }
   };
   if constexpr (SB) {
