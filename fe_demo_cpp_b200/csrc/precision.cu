@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <type_traits>
 
 #include "plan.hpp"
 #include "transpose_scatter.cuh"
@@ -30,6 +31,7 @@ Mat1D<P, Q, float> f32_mat(const BasisData& b) {
   Mat1D<P, Q, float> m;
   for (int i = 0; i < Q * P; ++i) m.B[i] = float(b.interp[i]), m.G[i] = float(b.grad[i]);
   for (int i = 0; i < Q; ++i) m.W[i] = float(b.q_weight[i]);
+  fill_eo(m);
   return m;
 }
 
@@ -45,12 +47,25 @@ constexpr int lowp_min_blocks() {
 template <class S>
 using LowpLauncher = void (*)(const MassPlan&, const S*, const S*, float*, float*, cudaStream_t);
 
-template <int P, int Q, class S>
+// The even-odd contractions (centro-symmetric B) where they measured faster in
+// single precision (interleaved A/B against the direct form, ~64M DoFs): 3D
+// P = 7 (FP32 1.21x, BF16 1.15x one component), P = 8 (1.04-1.07x) and BF16
+// at P = 6 (1.10x; FP32 there 0.82x); 2D only P = 8 (1.06-1.28x).
+template <int P, class S>
+constexpr bool lowp_even_odd_3d() {
+  return P >= 7 || (P == 6 && std::is_same<S, __nv_bfloat16>::value);
+}
+
+template <int P, int Q, class S, bool EO = lowp_even_odd_3d<P, S>() || P == 8>
 void launch_lowp(const MassPlan& p, const S* qd, const S* u, float* v, float* ev, cudaStream_t s) {
+  if constexpr (EO) {
+    if (!p.centro_symmetric) return launch_lowp<P, Q, S, false>(p, qd, u, v, ev, s);
+  }
+  constexpr bool eo3 = EO && lowp_even_odd_3d<P, S>(), eo2 = EO && P == 8;
   if (p.dim == 3) {
     using L = Mass3D<P, Q>;
     constexpr int smem = (L::SA + L::SB) * 4;
-    const auto kern = mass3d_apply_kernel<P, Q, lowp_min_blocks<P>(), float, ApplyPlain, 1, S>;
+    const auto kern = mass3d_apply_kernel<P, Q, lowp_min_blocks<P>(), float, ApplyPlain, 1, S, false, eo3>;
     static std::atomic<uint64_t> smem_set{0};
     set_smem(kern, smem, smem_set);
     const int64_t wave = resident_ctas(reinterpret_cast<const void*>(kern), L::NT, smem);  // L2 prefetch distance
@@ -59,7 +74,7 @@ void launch_lowp(const MassPlan& p, const S* qd, const S* u, float* v, float* ev
   } else if (p.dim == 2) {
     using L = Mass2D<P, Q>;
     constexpr int smem = (L::S1 + L::S3) * 4;
-    const auto kern = mass2d_apply_kernel<P, Q, float, ApplyPlain, S>;
+    const auto kern = mass2d_apply_kernel<P, Q, float, ApplyPlain, S, 0, false, eo2>;
     static std::atomic<uint64_t> smem_set{0};
     set_smem(kern, smem, smem_set);
     // no L2 prefetch in 2D reduced storage: measured mixed (BF16 at P = 2: 0.85-0.88x)
