@@ -64,12 +64,14 @@ __device__ __forceinline__ void with_matrix(const Mat1D<P, Q>& mp, F&& body) {
   }
 }
 
-// v[k][q][e] = (B x B x B) u[k][i][e]
-template <int P, int Q, bool SB = false>
+// v[k][q][e] = (B x B x B) u[k][i][e].  EO: the even-odd contractions
+// (eo_fwd; centro-symmetric B, the parameter matrix, not with SB).
+template <int P, int Q, bool SB = false, bool EO = false>
 __global__ void __launch_bounds__(Basis3D<P, Q>::NT) basis3d_interp_kernel(const __grid_constant__ Mat1D<P, Q> mp,
                                                                           const double* __restrict__ u,
                                                                           double* __restrict__ v, int num_elem,
                                                                           int num_comp) {
+  static_assert(!(SB && EO), "the even-odd folds live in the parameter matrix");
   with_matrix<SB>(mp, [&](const auto& m) {
   using L = Basis3D<P, Q>;
   constexpr int E = L::E;
@@ -86,12 +88,19 @@ __global__ void __launch_bounds__(Basis3D<P, Q>::NT) basis3d_interp_kernel(const
 #pragma unroll
       for (int pz = 0; pz < P; ++pz)
         x[pz] = valid ? __ldg(u + (int64_t(k) * L::P3 + (pz * P + py) * P + px) * ne + eg) : 0.0;
+      if constexpr (EO) {
+        double o[Q];
+        eo_fwd<P, Q>(m, x, o);
 #pragma unroll
-      for (int qz = 0; qz < Q; ++qz) {
-        double s = 0.0;
+        for (int qz = 0; qz < Q; ++qz) sa[py * L::PS1 + (qz * P + px) * E + e] = o[qz];
+      } else {
 #pragma unroll
-        for (int pz = 0; pz < P; ++pz) s += m.B[qz * P + pz] * x[pz];
-        sa[py * L::PS1 + (qz * P + px) * E + e] = s;
+        for (int qz = 0; qz < Q; ++qz) {
+          double s = 0.0;
+#pragma unroll
+          for (int pz = 0; pz < P; ++pz) s += m.B[qz * P + pz] * x[pz];
+          sa[py * L::PS1 + (qz * P + px) * E + e] = s;
+        }
       }
     }
     __syncthreads();
@@ -100,12 +109,19 @@ __global__ void __launch_bounds__(Basis3D<P, Q>::NT) basis3d_interp_kernel(const
       double y[P];
 #pragma unroll
       for (int py = 0; py < P; ++py) y[py] = sa[py * L::PS1 + col * E + e];
+      if constexpr (EO) {
+        double o[Q];
+        eo_fwd<P, Q>(m, y, o);
 #pragma unroll
-      for (int qy = 0; qy < Q; ++qy) {
-        double s = 0.0;
+        for (int qy = 0; qy < Q; ++qy) sb[px * L::PS2 + (qz * Q + qy) * E + e] = o[qy];
+      } else {
 #pragma unroll
-        for (int py = 0; py < P; ++py) s += m.B[qy * P + py] * y[py];
-        sb[px * L::PS2 + (qz * Q + qy) * E + e] = s;
+        for (int qy = 0; qy < Q; ++qy) {
+          double s = 0.0;
+#pragma unroll
+          for (int py = 0; py < P; ++py) s += m.B[qy * P + py] * y[py];
+          sb[px * L::PS2 + (qz * Q + qy) * E + e] = s;
+        }
       }
     }
     __syncthreads();
@@ -115,12 +131,20 @@ __global__ void __launch_bounds__(Basis3D<P, Q>::NT) basis3d_interp_kernel(const
 #pragma unroll
       for (int px = 0; px < P; ++px) w[px] = sb[px * L::PS2 + col * E + e];
       double* out = v + (int64_t(k) * L::Q3 + (qz * Q + qy) * Q) * ne + eg;
+      if constexpr (EO) {
+        double o[Q];
+        eo_fwd<P, Q>(m, w, o);
 #pragma unroll
-      for (int qx = 0; qx < Q; ++qx) {
-        double s = 0.0;
+        for (int qx = 0; qx < Q; ++qx)
+          if (valid) out[qx * ne] = o[qx];
+      } else {
 #pragma unroll
-        for (int px = 0; px < P; ++px) s += m.B[qx * P + px] * w[px];
-        if (valid) out[qx * ne] = s;
+        for (int qx = 0; qx < Q; ++qx) {
+          double s = 0.0;
+#pragma unroll
+          for (int px = 0; px < P; ++px) s += m.B[qx * P + px] * w[px];
+          if (valid) out[qx * ne] = s;
+        }
       }
     }
     // the next component's A writes sa, last read by B before the barrier
@@ -129,12 +153,14 @@ __global__ void __launch_bounds__(Basis3D<P, Q>::NT) basis3d_interp_kernel(const
   });
 }
 
-// v[k][i][e] = (B^T x B^T x B^T) u[k][q][e]
-template <int P, int Q, bool SB = false>
+// v[k][i][e] = (B^T x B^T x B^T) u[k][q][e].  EO: the even-odd contractions
+// (eo_bwd), as for interp.
+template <int P, int Q, bool SB = false, bool EO = false>
 __global__ void __launch_bounds__(Basis3D<P, Q>::NT) basis3d_interp_t_kernel(const __grid_constant__ Mat1D<P, Q> mp,
                                                                             const double* __restrict__ u,
                                                                             double* __restrict__ v, int num_elem,
                                                                             int num_comp) {
+  static_assert(!(SB && EO), "the even-odd folds live in the parameter matrix");
   with_matrix<SB>(mp, [&](const auto& m) {
   using L = Basis3D<P, Q>;
   constexpr int E = L::E;
@@ -151,12 +177,19 @@ __global__ void __launch_bounds__(Basis3D<P, Q>::NT) basis3d_interp_t_kernel(con
       double r[Q];
 #pragma unroll
       for (int qx = 0; qx < Q; ++qx) r[qx] = valid ? __ldg(in + qx * ne) : 0.0;
+      if constexpr (EO) {
+        double o[P];
+        eo_bwd<P, Q>(m, r, o);
 #pragma unroll
-      for (int px = 0; px < P; ++px) {
-        double s = 0.0;
+        for (int px = 0; px < P; ++px) sa[qy * L::PS3 + (qz * P + px) * E + e] = o[px];
+      } else {
 #pragma unroll
-        for (int qx = 0; qx < Q; ++qx) s += m.B[qx * P + px] * r[qx];
-        sa[qy * L::PS3 + (qz * P + px) * E + e] = s;
+        for (int px = 0; px < P; ++px) {
+          double s = 0.0;
+#pragma unroll
+          for (int qx = 0; qx < Q; ++qx) s += m.B[qx * P + px] * r[qx];
+          sa[qy * L::PS3 + (qz * P + px) * E + e] = s;
+        }
       }
     }
     __syncthreads();
@@ -165,12 +198,19 @@ __global__ void __launch_bounds__(Basis3D<P, Q>::NT) basis3d_interp_t_kernel(con
       double y[Q];
 #pragma unroll
       for (int qy = 0; qy < Q; ++qy) y[qy] = sa[qy * L::PS3 + col * E + e];
+      if constexpr (EO) {
+        double o[P];
+        eo_bwd<P, Q>(m, y, o);
 #pragma unroll
-      for (int py = 0; py < P; ++py) {
-        double s = 0.0;
+        for (int py = 0; py < P; ++py) sb[qz * L::PS4 + (py * P + px) * E + e] = o[py];
+      } else {
 #pragma unroll
-        for (int qy = 0; qy < Q; ++qy) s += m.B[qy * P + py] * y[qy];
-        sb[qz * L::PS4 + (py * P + px) * E + e] = s;
+        for (int py = 0; py < P; ++py) {
+          double s = 0.0;
+#pragma unroll
+          for (int qy = 0; qy < Q; ++qy) s += m.B[qy * P + py] * y[qy];
+          sb[qz * L::PS4 + (py * P + px) * E + e] = s;
+        }
       }
     }
     __syncthreads();
@@ -178,11 +218,17 @@ __global__ void __launch_bounds__(Basis3D<P, Q>::NT) basis3d_interp_t_kernel(con
       double z[Q];
 #pragma unroll
       for (int qz = 0; qz < Q; ++qz) z[qz] = sb[qz * L::PS4 + col * E + e];
+      double zo[P];
+      if constexpr (EO) eo_bwd<P, Q>(m, z, zo);
 #pragma unroll
       for (int pz = 0; pz < P; ++pz) {
         double s = 0.0;
+        if constexpr (EO) {
+          s = zo[pz];
+        } else {
 #pragma unroll
-        for (int qz = 0; qz < Q; ++qz) s += m.B[qz * P + pz] * z[qz];
+          for (int qz = 0; qz < Q; ++qz) s += m.B[qz * P + pz] * z[qz];
+        }
         if (valid) v[(int64_t(k) * L::P3 + pz * P * P + col) * ne + eg] = s;
       }
     }
