@@ -60,18 +60,30 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic():
-    """DRAM bytes per launch of the fused kernel from the committed ncu summary
-    (profiles/mass3d_apply_P5Q6_64M.md, line 'dram_bytes_per_launch: <n>')."""
-    path = os.path.join(ROOT, "profiles", "mass3d_apply_P5Q6_64M.md")
+TRAFFIC_PROFILE = os.path.join("profiles", "mass3d_apply_P5Q6_64M.md")
+
+
+def ncu_traffic(variant):
+    """DRAM bytes per launch of the fused kernel as captured by ncu and
+    summarised in profiles/mass3d_apply_P5Q6_64M.md (line
+    'dram_bytes_per_launch: <n> (<variant>)'), labelled as that profile's
+    figure: it is not measured in this run.  None when the profile covers
+    another kernel variant than the one this run times."""
+    path = os.path.join(ROOT, TRAFFIC_PROFILE)
     if not os.path.exists(path):
         return None
     for line in open(path):
         if line.strip().startswith("dram_bytes_per_launch:"):
+            rest = line.split(":", 1)[1].strip()
             try:
-                return float(line.split(":", 1)[1].strip().split()[0])
+                val = float(rest.split()[0])
             except ValueError:
                 return None
+            tag = rest[rest.find("(") + 1: rest.find(")")] if "(" in rest else ""
+            if tag and tag != variant:
+                return None
+            return {"value": val, "source": f"ncu capture of the same workload, {TRAFFIC_PROFILE} "
+                                          "(not measured in this run)"}
     return None
 
 
@@ -151,6 +163,7 @@ def run_reference(args, rank):
     s.close()
     t = statistics.median(times)
     value = s.gdofs(t)
+    single = single_core_baseline(mesh)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
@@ -158,10 +171,22 @@ def run_reference(args, rank):
         "config": {"workload": WORKLOAD, "mesh": "x".join(map(str, SHAPE)), "P": P, "Q": Q, "num_comp": NC,
                    "dofs": mesh.num_nodes, "parallelism": "host threads over element chunks"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": s.threads, "kind": "reference",
-                         "sample": s.describe()},
+                         "sample": s.describe(), "single_core": single},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     return line
+
+
+def single_core_baseline(mesh, target_s=3.0):
+    """The reference operator_apply on one host thread (it is single-threaded,
+    src/operator.cpp:148), on a bounded sample of whole z-slabs: median of 3
+    after 1 warm-up, GDoF/s scaled to the workload by the element fraction."""
+    s = RefSample(mesh, target_s=target_s, threads=1)
+    s._time_once()
+    ts = [s._time_once() for _ in range(3)]
+    s.close()
+    return {"value": s.gdofs(statistics.median(ts)), "unit": UNIT, "cores": 1, "kind": "reference",
+            "sample": s.describe() + ", median of 3 after 1 warm-up"}
 
 
 # ---------------------------------------------------------------------------
@@ -269,7 +294,7 @@ def run_b200(args, rank, world, local_rank):
     peak, peak_kind = measured_peaks()
     abytes = algorithmic_bytes(ne, N, P, Q)
     achieved = abytes / (t_kern * 1e-3) / 1e9
-    traffic = ncu_traffic()
+    traffic = ncu_traffic(info["kernel"]) if (SHAPE, P) == ((100, 100, 100), 5) else None
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup,
         "ms_per_step": t_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -290,14 +315,81 @@ def run_b200(args, rank, world, local_rank):
         "clocks": clocks,
         "gpu_launches": 2 * K * launches,
     }
+    if rank == 0 and world == 1 and not args.no_orders:
+        # after the timed region and the e2e run; the workload's buffers are released first
+        del u, v, w, op, ru, bu
+        torch.cuda.empty_cache()
+        line["orders"] = {"note": "P = 2..4 (Q = P+1), ~64M DoFs, FP64, atomic scatter, autotuned kernel; "
+                                  "kernel_ms = the fused kernel alone (apply_add), apply_ms = the public apply "
+                                  "(v zeroed + kernel); frac = algorithmic bytes / kernel_ms / measured HBM peak; "
+                                  f"{args.orders_steps} launches each, CUDA events",
+                          "entries": measure_orders(dev, peak, args.orders_steps)}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         s = RefSample(mesh, target_s=args.cpu_sample_s / 4)
         s._time_once()
         ts = [s._time_once() for _ in range(3)]
         s.close()
         line["cpu_baseline"] = {"value": s.gdofs(statistics.median(ts)), "unit": UNIT, "cores": s.threads,
-                                "kind": "reference", "sample": s.describe() + ", median of 3 after 1 warm-up"}
+                                "kind": "reference", "sample": s.describe() + ", median of 3 after 1 warm-up",
+                                "single_core": single_core_baseline(mesh)}
     return line
+
+
+# ---------------------------------------------------------------------------
+# low orders in the same run: P = 2, 3, 4 (Q = P+1) at ~64M DoFs, one and three
+# components (the vector mass), the plan's autotuned kernel; the fused FP64
+# apply's HBM roofline fraction at each
+# ---------------------------------------------------------------------------
+ORDERS = [(2, 1), (2, 3), (3, 1), (3, 3), (4, 1), (4, 3)]
+
+
+def measure_orders(dev, peak, steps):
+    import torch
+    import fe_demo_cpp_b200 as fem
+    from fe_demo_cpp_b200.mesh import mesh_for_dofs
+    from fe_demo_cpp_b200.mesh_gpu import box_mesh_device
+
+    out = []
+    for Pp, nc in ORDERS:
+        Qq = Pp + 1
+        shape = mesh_for_dofs(64_000_000 // nc, Pp, 3)
+        m = box_mesh_device(shape, Pp, seed=SEED, device=dev)
+        N, ne = m.num_nodes, m.num_elem
+        offs = m.offsets.cpu().numpy()
+        rx = fem.Restriction(ne, Pp**3, 3, N, 3 * N, offs)
+        qd = torch.empty(Qq**3 * ne, dtype=torch.float64, device=dev)
+        fem.mass_build(rx, fem.Basis(3, 3, Pp, Qq), m.coords, qd)
+        del rx
+        m.coords = None
+        op = fem.MassOperator(fem.Restriction(ne, Pp**3, nc, N, nc * N, offs), fem.Basis(3, nc, Pp, Qq), qd,
+                              fem.QF.apply_mass_vector if nc > 1 else fem.QF.apply_mass)
+        del qd
+        g = torch.Generator(device=dev).manual_seed(SEED)
+        u = torch.rand(nc * N, dtype=torch.float64, device=dev, generator=g) * 2 - 1
+        v = torch.empty_like(u)
+        op.autotune(u, v, reps=5)
+        variant = op.info()["kernel"]
+        for _ in range(3):
+            op.apply(u, v)
+        res = {}
+        for name, fn in (("apply", op.apply), ("kernel", op.apply_add)):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            for _ in range(steps):
+                fn(u, v)
+            e1.record()
+            torch.cuda.synchronize()
+            res[name] = e0.elapsed_time(e1) / steps
+        ab = algorithmic_bytes(ne, N, Pp, Qq, nc)
+        out.append({"P": Pp, "Q": Qq, "num_comp": nc, "mesh": "x".join(map(str, shape)), "dofs": nc * N,
+                    "kernel_variant": variant, "apply_ms": res["apply"], "kernel_ms": res["kernel"],
+                    "gdofs": nc * N / res["apply"] / 1e6, "algorithmic_bytes": ab,
+                    "frac": ab / (res["kernel"] * 1e-3) / 1e9 / peak,
+                    "frac_apply": ab / (res["apply"] * 1e-3) / 1e9 / peak})
+        del op, u, v, m
+        torch.cuda.empty_cache()
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -880,6 +972,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-orders", action="store_true", help="skip the P = 2..4 roofline fractions")
+    ap.add_argument("--orders-steps", type=int, default=20)
     ap.add_argument("--cpu-sample-s", type=float, default=12.0, help="approximate CPU seconds of the baseline")
     ap.add_argument("--shape", default=None, help="elements per direction nx,ny,nz (default 100,100,100)")
     ap.add_argument("--P", type=int, default=None, help="nodes per direction (Q = P+1)")

@@ -232,6 +232,22 @@ class Basis(_Handle):
         call("fem_b200_basis_create", dim, num_comp, P, Q, int(quad_mode), C.addressof(self.h))
         self.dim, self.num_comp, self.P, self.Q, self.quad_mode = dim, num_comp, P, Q, QuadMode(quad_mode)
 
+    @classmethod
+    def from_matrices(cls, dim, num_comp, P, Q, q_weight_1d, interp_1d, grad_1d):
+        """A basis from caller-given 1D data (q_weight_1d[Q], interp_1d and
+        grad_1d [Q][P] row-major), as the reference's TensorBasis whose fields
+        the caller filled in (include/basis.hpp:28-40)."""
+        self = cls.__new__(cls)
+        _Handle.__init__(self)
+        w = np.ascontiguousarray(q_weight_1d, dtype=np.float64)
+        B = np.ascontiguousarray(interp_1d, dtype=np.float64)
+        G = np.ascontiguousarray(grad_1d, dtype=np.float64)
+        if w.size != Q or B.size != Q * P or G.size != Q * P:
+            raise ValueError("Basis.from_matrices: q_weight_1d needs Q entries, interp_1d and grad_1d Q*P")
+        call("fem_b200_basis_create_from", dim, num_comp, P, Q, _ptr(w), _ptr(B), _ptr(G), C.addressof(self.h))
+        self.dim, self.num_comp, self.P, self.Q, self.quad_mode = dim, num_comp, P, Q, None
+        return self
+
     def host_data(self):
         return tensor_h1_lagrange(self.dim, self.num_comp, self.P, self.Q, self.quad_mode)
 

@@ -695,9 +695,11 @@ int fem_b200_basis_apply(fem_b200_basis b, int num_elem, int t_mode, int eval_mo
   });
 }
 
-// Same contractions as fem_b200_basis_apply, with the pass buffers in
-// g_basis_static_scratch: nothing is allocated.  Each pass overwrites the
-// scratch it writes, so nothing has to be cleared between calls.
+// Same contractions as fem_b200_basis_apply: dim 3 first through the fused
+// one-pass kernels (no scratch at all, no size limit), otherwise the generic
+// passes with their buffers in g_basis_static_scratch.  Nothing is allocated.
+// Each pass overwrites the scratch it writes, so nothing has to be cleared
+// between calls; the scratch address is looked up only when a call uses it.
 int fem_b200_basis_apply_static(fem_b200_basis b, int num_elem, int t_mode, int eval_mode, const double* u,
                                 int64_t n_u, double* v, int64_t n_v, void* stream) {
   return guarded([&] {
@@ -725,6 +727,8 @@ int fem_b200_basis_apply_static(fem_b200_basis b, int num_elem, int t_mode, int 
     const int64_t out_n = tr ? pn : (grad ? h.dim * qn : qn);
     require(n_u == in_n && u, "tensor_basis_apply: u has the wrong size");
     require(n_v == out_n && v, "tensor_basis_apply: v has the wrong size");
+    // dim 3: one fused pass, no scratch (the same kernels as fem_b200_basis_apply)
+    if (basis3d_fused_apply(h, num_elem, tr, grad, u, v, s)) return;
     const int P = tr ? h.Q : h.P, Q = tr ? h.P : h.Q;
     const int64_t big = h.num_comp * ipow(std::max(h.P, h.Q), h.dim) * num_elem;
     const int64_t need = h.dim > 1 ? 2 * big : 0;
@@ -732,8 +736,8 @@ int fem_b200_basis_apply_static(fem_b200_basis b, int num_elem, int t_mode, int 
       throw arg_error("tensor_basis_apply (static scratch): this call needs " + std::to_string(need) +
                       " doubles of scratch (2 * num_comp * max(P,Q)^dim * num_elem) but the static scratch holds " +
                       std::to_string(kStaticScratchDoubles) + " (16 MiB); split the elements into smaller calls");
-    double* scratch = static_scratch_on(bd.device);
-    double* tmp[2] = {scratch, scratch + big};
+    double* scratch = need > 0 ? static_scratch_on(bd.device) : nullptr;  // dim 1 passes use no scratch
+    double* tmp[2] = {scratch, scratch ? scratch + big : nullptr};
     const int naxes = grad ? h.dim : 1;
     for (int ax = 0; ax < naxes; ++ax) {
       int64_t pre = h.num_comp * ipow(P, h.dim - 1), post = num_elem;

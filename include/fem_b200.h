@@ -186,13 +186,16 @@ int fem_b200_basis_apply(fem_b200_basis b, int num_elem, int t_mode, int eval_mo
  * CUDA graph (cudaMalloc is not permitted during a global-mode capture), hosts
  * whose device memory is owned by another allocator or a fixed budget, and
  * loops that must not stall on the allocator.  This entry point takes the same
- * arguments and computes the same result, with the pass buffers in a fixed
- * array compiled into the library: 2,097,152 doubles (16 MiB), which every
- * GPU that loads the library holds until the process exits.  A call needing
- * more (2 * num_comp * max(P,Q)^dim * num_elem doubles for dim > 1) fails with
- * FEM_B200_ERROR_ARGUMENT; split the elements over several calls.  The first
- * call on a device looks up the array's device address (set-up that may load
- * the module), so make that first call before any stream capture.  All calls
+ * arguments and computes the same result without allocating.  Dimension 3 runs
+ * the fused one-pass kernels, which use no scratch (no size limit).  Other
+ * shapes run the generic passes with their buffers in a fixed array compiled
+ * into the library: 2,097,152 doubles (16 MiB), which every GPU that loads the
+ * library holds until the process exits.  A call needing more
+ * (2 * num_comp * max(P,Q)^dim * num_elem doubles for dim 2, or dim 3 without a
+ * fused kernel) fails with FEM_B200_ERROR_ARGUMENT; split the elements over
+ * several calls.  The first call on a device that uses the array looks up its
+ * device address (set-up that may load the module), so make that first call
+ * before any stream capture.  All calls
  * share the one array: calls that overlap on the GPU (other streams, other
  * host threads) race and must be serialised by the caller.  Each pass
  * overwrites the scratch it uses, so nothing needs clearing between calls. */

@@ -31,7 +31,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_lib", "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libfemref.so")
 REFCUDA_SO = os.path.join(HERE, "_ref", "libfemrefcuda.so")
-REF_SOURCE = "/root/reference"
+# The fe-demo-cpp source tree the reference build compiles from: the
+# FE_DEMO_CPP_SRC environment variable, else its checkout location on the
+# build container.  Absent on machines that only run the prebuilt libraries.
+REF_SOURCE = os.environ.get("FE_DEMO_CPP_SRC", "/root/reference")
 
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
@@ -43,6 +46,9 @@ def build(with_ref: bool | None = None) -> None:
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
     if with_ref is None:
         with_ref = os.path.isdir(os.path.join(REF_SOURCE, "src"))
+    elif with_ref and not os.path.isdir(os.path.join(REF_SOURCE, "src")):
+        raise FileNotFoundError(f"oracle: fe-demo-cpp sources not found at {REF_SOURCE!r} "
+                                "(set FE_DEMO_CPP_SRC to the source tree)")
     if with_ref:
         subprocess.run(["make", "-s", "-C", HERE, "ref", "refcuda", f"REF={REF_SOURCE}"], check=True)
 
@@ -170,10 +176,15 @@ class _Orc:
             raise RuntimeError("orc_mass_build failed")
         return qd
 
-    def mass_apply(self, dim, ne, P, Q, nc, comp_stride, l_size, offsets, qdata, u, quad_mode=0, vector=False):
+    def mass_apply(self, dim, ne, P, Q, nc, comp_stride, l_size, offsets, qdata, u, quad_mode=0, vector=False,
+                   interp_1d=None):
         """v = M u.  vector=False: the reference apply_mass (component 0 only
-        for nc > 1); vector=True: every component (nc scalar applies)."""
+        for nc > 1); vector=True: every component (nc scalar applies).
+        interp_1d: a caller-given [Q][P] interpolation matrix in place of the
+        Lagrange basis's."""
         _, _, B, _ = self.basis(dim, nc, P, Q, quad_mode)
+        if interp_1d is not None:
+            B = _f64(interp_1d).reshape(B.shape)
         v = np.zeros(l_size)
         if vector:
             rc = self.L.orc_mass_apply_vector(dim, ne, P, Q, nc, comp_stride, l_size, _i32(offsets), B, _f64(qdata),

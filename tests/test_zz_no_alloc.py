@@ -7,8 +7,10 @@ same thing with its buffers in a fixed 16 MiB device array compiled into the
 library.  Here it is called through the C ABI twice in a row and compared with
 the allocating entry point, at the tolerance of the other device tests
 (normwise 1e-13), and a call that needs more than the array holds must fail
-with an argument error.  This file runs last so that a failure here cannot
-stop the rest of the suite.
+with an argument error.  Dimension-3 calls run the fused one-pass kernels,
+which need no scratch, so they are not bounded by the array (the 2000-element
+case below would need 2,592,000 doubles through the generic passes).  This
+file runs last so that a failure here cannot stop the rest of the suite.
 """
 import ctypes as C
 
@@ -25,7 +27,7 @@ def _close(got, want):
     assert err <= TOL, f"normwise relative error {err:.3e} > {TOL:.0e}"
 
 
-CASES = [(3, 3, 5, 6, 40), (3, 1, 4, 5, 100), (2, 2, 3, 4, 50), (1, 1, 6, 7, 30)]
+CASES = [(3, 3, 5, 6, 40), (3, 3, 5, 6, 2000), (3, 1, 4, 5, 100), (2, 2, 3, 4, 50), (1, 1, 6, 7, 30)]
 
 
 @pytest.mark.parametrize("dim,nc,P,Q,ne", CASES)
@@ -61,11 +63,11 @@ def test_static_scratch_rejects_sizes_beyond_its_maximum(fem, cuda):
     from fe_demo_cpp_b200 import _lib
     lib = _lib.load()
     b = C.c_void_p()
-    _lib.check(lib.fem_b200_basis_create(3, 3, 5, 6, 0, C.byref(b)))
+    _lib.check(lib.fem_b200_basis_create(2, 3, 5, 6, 0, C.byref(b)))
     try:
-        ne = 2000  # needs 2 * 3 * 6^3 * 2000 = 2,592,000 doubles > 2,097,152
-        u = torch.zeros(3 * 125 * ne, dtype=torch.float64, device=cuda)
-        v = torch.zeros(3 * 216 * ne, dtype=torch.float64, device=cuda)
+        ne = 10000  # dim 2 runs the generic passes: 2 * 3 * 6^2 * 10000 = 2,160,000 doubles > 2,097,152
+        u = torch.zeros(3 * 25 * ne, dtype=torch.float64, device=cuda)
+        v = torch.zeros(3 * 36 * ne, dtype=torch.float64, device=cuda)
         rc = lib.fem_b200_basis_apply_static(b, ne, 0, 1, u.data_ptr(), u.numel(), v.data_ptr(), v.numel(),
                                              torch.cuda.current_stream().cuda_stream)
         assert rc == _lib.ERROR_ARGUMENT
