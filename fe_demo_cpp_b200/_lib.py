@@ -61,6 +61,9 @@ SIGNATURES = {
     "fem_b200_mass_apply_host": ([_p, _p, _i64, _p, _i64, _p], _i),
     "fem_b200_mass_info": ([_p, _p, _p, _p, _p], _i),
     "fem_b200_mass_set_kernel": ([_p, _i], _i),
+    "fem_b200_mass_apply_f32_tc": ([_p, _p, _i64, _p, _i64, _i, _p], _i),
+    "fem_b200_mass_apply_bf16_tc": ([_p, _p, _i64, _p, _i64, _p], _i),
+    "fem_b200_tc_selftest": ([_p], _i),
     "fem_b200_mass_set_host_chunks": ([_p, _i], _i),
     "fem_b200_mass_check": ([_p, _p], _i),
     "fem_b200_mass_diagonal": ([_p, _p, _i64, _p], _i),

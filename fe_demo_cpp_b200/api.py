@@ -324,6 +324,20 @@ class MassOperator(_Handle):
         _check_dev(v, "float32")
         call("fem_b200_mass_apply_f32", self.h, _ptr(u), _n(u), _ptr(v), _n(v), _stream(stream))
 
+    def apply_f32_tc(self, u, v, split=True, stream=None):
+        """v = M u in FP32 storage with the 1D contractions on the tensor cores
+        (TF32 inputs, FP32 accumulation; split: 3xTF32, FP32-level accuracy)."""
+        _check_dev(u, "float32")
+        _check_dev(v, "float32")
+        call("fem_b200_mass_apply_f32_tc", self.h, _ptr(u), _n(u), _ptr(v), _n(v), 1 if split else 0,
+             _stream(stream))
+
+    def apply_bf16_tc(self, u, v, stream=None):
+        """v (float32) = M u, u (bfloat16) and qdata in BF16, contractions on the tensor cores."""
+        _check_dev(u, "bfloat16")
+        _check_dev(v, "float32")
+        call("fem_b200_mass_apply_bf16_tc", self.h, _ptr(u), _n(u), _ptr(v), _n(v), _stream(stream))
+
     def apply_bf16(self, u, v, stream=None):
         """v (float32) = M u with u (bfloat16) and qdata in BF16 storage, FP32 arithmetic."""
         _check_dev(u, "bfloat16")

@@ -8,8 +8,10 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <cstring>
 #include <type_traits>
 
+#include "mass_tc.cuh"
 #include "plan.hpp"
 #include "transpose_scatter.cuh"
 
@@ -115,26 +117,126 @@ const LowpDispatch& lowp_dispatch() {
   return d;
 }
 
-// v = M u with u, qdata in S and v in FP32
+// The plan's tiled qdata in storage S, converted from the FP64 copy on first use.
 template <class S>
-void lowp_apply(MassPlan& p, const S* u, float* v, cudaStream_t s) {
+const S* lowp_qdata(MassPlan& p, cudaStream_t s) {
   const size_t nq = p.qd_t.size();
-  const S* qd = nullptr;
   if constexpr (std::is_same<S, float>::value) {
     if (p.qd_t32.size() != nq) {
       p.qd_t32.alloc(nq);
       qdata_to_f32_kernel<<<grid_for(int64_t(nq), 256), 256, 0, s>>>(int64_t(nq), p.qd_t.get(), p.qd_t32.get());
       FEM_LAUNCH_CHECK();
     }
-    qd = p.qd_t32.get();
+    return p.qd_t32.get();
   } else {
     if (p.qd_t16.size() != nq) {
       p.qd_t16.alloc(nq);
       qdata_to_bf16_kernel<<<grid_for(int64_t(nq), 256), 256, 0, s>>>(int64_t(nq), p.qd_t.get(), p.qd_t16.get());
       FEM_LAUNCH_CHECK();
     }
-    qd = p.qd_t16.get();
+    return p.qd_t16.get();
   }
+}
+
+// ---- tensor-core applies (mass_tc.cuh) --------------------------------------
+// TF32 rounding on the host (nearest, ties away: cvt.rna's rule).
+float host_tf32(float x) {
+  uint32_t w;
+  std::memcpy(&w, &x, 4);
+  w = (w + 0x1000u) & 0xFFFFE000u;
+  float y;
+  std::memcpy(&y, &w, 4);
+  return y;
+}
+
+// The B operands of the tensor-core kernel from the FP64 interpolation matrix:
+// forward n = q, k = p (B[q][p]); backward n = p, k = q (B[q][p] too); rows
+// 0-7 the TF32 part, rows 8-15 the TF32 part of the remainder (split) or 0.
+TcMats tc_mats(const BasisData& b) {
+  TcMats m;
+  std::memset(&m, 0, sizeof(m));
+  for (int n = 0; n < 8; ++n)
+    for (int k = 0; k < 8; ++k) {
+      for (int dir = 0; dir < 2; ++dir) {
+        const int q = dir == 0 ? n : k, pp = dir == 0 ? k : n;
+        if (q >= b.Q || pp >= b.P) continue;
+        const double x = b.interp[size_t(q * b.P + pp)];
+        const float hi = host_tf32(float(x));
+        const float lo = host_tf32(float(x - double(hi)));
+        m.op[2 * dir][tc::kmajor_index(n, k)] = hi;
+        m.op[2 * dir][tc::kmajor_index(n + 8, k)] = lo;
+        m.op[2 * dir + 1][tc::kmajor_index(n, k)] = hi;
+      }
+    }
+  return m;
+}
+
+template <class S>
+using TcLauncher = void (*)(const MassPlan&, const S*, const S*, float*, cudaStream_t);
+
+template <int P, int Q, bool SPLIT, class S>
+void launch_tc(const MassPlan& p, const S* qd, const S* u, float* v, cudaStream_t s) {
+  using L = TcMass3D<P, Q>;
+  constexpr int smem = L::smem(SPLIT);
+  const auto kern = mass3d_apply_tc_kernel<P, Q, SPLIT, S>;
+  static std::atomic<uint64_t> smem_set{0};
+  set_smem(kern, smem, smem_set);
+  const int grid = int(std::min<int64_t>(p.n_tiles, resident_ctas(reinterpret_cast<const void*>(kern), L::NT, smem)));
+  kern<<<grid, L::NT, smem, s>>>(tc_mats(p.basis), p.offs_t.get(), qd, u, v, p.num_elem, p.comp_run, p.comp_stride,
+                                 p.n_tiles, p.status.get());
+  FEM_LAUNCH_CHECK();
+}
+
+constexpr int kTcMinP = 6;
+
+struct TcDispatch {
+  TcLauncher<float> f32_split[kMaxP + 1][kQSpan] = {};
+  TcLauncher<float> f32[kMaxP + 1][kQSpan] = {};
+  TcLauncher<__nv_bfloat16> bf16[kMaxP + 1][kQSpan] = {};
+  template <int P, int DQ>
+  void fill() {
+    constexpr int Q = P + DQ;
+    if constexpr (Q <= 8) {
+      f32_split[P][DQ] = launch_tc<P, Q, true, float>;
+      f32[P][DQ] = launch_tc<P, Q, false, float>;
+      bf16[P][DQ] = launch_tc<P, Q, false, __nv_bfloat16>;
+    }
+    if constexpr (DQ + 1 < kQSpan)
+      fill<P, DQ + 1>();
+    else if constexpr (P + 1 <= kMaxP)
+      fill<P + 1, 0>();
+  }
+  TcDispatch() { fill<kTcMinP, 0>(); }
+};
+
+const TcDispatch& tc_dispatch() {
+  static TcDispatch d;
+  return d;
+}
+
+// v = M u on the tensor cores: u, qdata in S, v in FP32; split: the 3xTF32
+// form (FP32 storage only).
+template <class S>
+void tc_apply(MassPlan& p, const S* u, float* v, bool split, cudaStream_t s) {
+  if (p.dim != 3 || p.P < kTcMinP || p.P > kMaxP || p.Q < p.P || p.Q > 8)
+    throw unsupported_error("tensor-core apply: no kernel for " + shape_str(p.dim, p.P, p.Q) +
+                            " (dim 3, P = 6..8, Q = P..8)");
+  if (p.scatter_mode != FEM_B200_SCATTER_ATOMIC)
+    throw unsupported_error("tensor-core apply: atomic scatter only");
+  TcLauncher<S> launch = nullptr;
+  if constexpr (std::is_same<S, float>::value)
+    launch = split ? tc_dispatch().f32_split[p.P][p.Q - p.P] : tc_dispatch().f32[p.P][p.Q - p.P];
+  else
+    launch = tc_dispatch().bf16[p.P][p.Q - p.P];
+  const S* qd = lowp_qdata<S>(p, s);
+  FEM_CUDA_CHECK(cudaMemsetAsync(v, 0, size_t(p.l_size) * sizeof(float), s));
+  launch(p, qd, u, v, s);
+}
+
+// v = M u with u, qdata in S and v in FP32
+template <class S>
+void lowp_apply(MassPlan& p, const S* u, float* v, cudaStream_t s) {
+  const S* qd = lowp_qdata<S>(p, s);
   FEM_CUDA_CHECK(cudaMemsetAsync(v, 0, size_t(p.l_size) * sizeof(float), s));
   const LowpDispatch& d = lowp_dispatch();
   LowpLauncher<S> launch = nullptr;
@@ -169,6 +271,30 @@ int fem_b200_mass_apply_f32(fem_b200_mass op, const float* u, int64_t n_u, float
     require(n_v == p.l_size && v, "operator_apply: output vector size does not match active_out_l_size");
     DeviceGuard g(p.device);
     lowp_apply<float>(p, u, v, as_stream(stream));
+  });
+}
+
+int fem_b200_mass_apply_f32_tc(fem_b200_mass op, const float* u, int64_t n_u, float* v, int64_t n_v, int split,
+                               void* stream) {
+  return guarded([&] {
+    require(op && op->d, "operator_apply: NULL handle");
+    MassPlan& p = *op->d;
+    require(n_u == p.l_size && u, "operator_apply: input vector size does not match active_in_l_size");
+    require(n_v == p.l_size && v, "operator_apply: output vector size does not match active_out_l_size");
+    require(split == 0 || split == 1, "tensor-core apply: split must be 0 or 1");
+    DeviceGuard g(p.device);
+    tc_apply<float>(p, u, v, split == 1, as_stream(stream));
+  });
+}
+
+int fem_b200_mass_apply_bf16_tc(fem_b200_mass op, const void* u, int64_t n_u, float* v, int64_t n_v, void* stream) {
+  return guarded([&] {
+    require(op && op->d, "operator_apply: NULL handle");
+    MassPlan& p = *op->d;
+    require(n_u == p.l_size && u, "operator_apply: input vector size does not match active_in_l_size");
+    require(n_v == p.l_size && v, "operator_apply: output vector size does not match active_out_l_size");
+    DeviceGuard g(p.device);
+    tc_apply<__nv_bfloat16>(p, static_cast<const __nv_bfloat16*>(u), v, false, as_stream(stream));
   });
 }
 

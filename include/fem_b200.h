@@ -446,6 +446,27 @@ int fem_b200_mass_apply_f32(fem_b200_mass op, const float *u, int64_t n_u, float
 int fem_b200_mass_apply_bf16(fem_b200_mass op, const void *u_bf16, int64_t n_u, float *v, int64_t n_v,
                              void *stream);
 
+/* operator_apply with its 1D contractions on the tensor cores (tcgen05.mma,
+ * TF32 inputs, FP32 accumulation; src/operator.cpp:148-182 computes in FP64
+ * with scalar loops, src/tensor-contract.cpp:35-91).  3D plans with P = 6..8,
+ * Q = P..8 and atomic scatter (else FEM_B200_ERROR_UNSUPPORTED).
+ * _f32_tc: u, v, qdata FP32; split = 1 stages every operand as two TF32
+ * parts (3xTF32: FP32-level accuracy), split = 0 as one (relative rounding
+ * 2^-11 per contraction).  _bf16_tc: u and qdata BF16, one TF32 part.  v is
+ * overwritten; device pointers, `stream` order. */
+int fem_b200_mass_apply_f32_tc(fem_b200_mass op, const float *u, int64_t n_u, float *v, int64_t n_v, int split,
+                               void *stream);
+int fem_b200_mass_apply_bf16_tc(fem_b200_mass op, const void *u_bf16, int64_t n_u, float *v, int64_t n_v,
+                                void *stream);
+
+/* Self-test of the tensor-core layer behind the _tc applies (no counterpart
+ * in the reference): one M = 128, N = 16, K = 8 TF32 tcgen05.mma with the
+ * operands staged as the applies stage them, read back from tensor memory;
+ * writes max |D - A B^T| / max |A B^T| against the host product of the
+ * TF32-rounded inputs (FP32 rounding of the sums, ~1e-7, when the
+ * descriptors and layouts are right). */
+int fem_b200_tc_selftest(double *max_rel_err);
+
 /* Synchronise `stream` and report a device-side failure of the plan's kernels
  * (a bounded wait that ran out) as FEM_B200_ERROR_CUDA.  fem_b200_mass_apply_host
  * does this check itself. */
