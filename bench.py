@@ -410,7 +410,7 @@ def run_sweep(args):
     for dim, Pp in [(d, p) for d in (int(x) for x in args.sweep_dim.split(",")) for p in Ps]:
         Qq = Pp + 1
         for nc in (1, 3):
-            shape = mesh_for_dofs(64_000_000 // nc, Pp, dim)
+            shape = mesh_for_dofs(args.sweep_dofs // nc, Pp, dim)
             m = box_mesh_device(shape, Pp, seed=SEED, device=dev)
             N, ne = m.num_nodes, m.num_elem
             offs = m.offsets.cpu().numpy()
@@ -427,7 +427,7 @@ def run_sweep(args):
             v = torch.empty_like(u)
             abytes = algorithmic_bytes(ne, N, Pp, Qq, nc, dim)
             for variant in fem.KernelVariant:
-                if variant == fem.KernelVariant.auto:
+                if variant == fem.KernelVariant.auto or args.sweep_storage_only:
                     continue
                 try:
                     op.set_kernel(variant)
@@ -450,13 +450,18 @@ def run_sweep(args):
                                   "roofline_frac": abytes / (kms * 1e-3) / 1e9 / peak,
                                   "fp64_tflops": algorithmic_flops(ne, Pp, Qq, nc, dim) / (kms * 1e-3) / 1e12}),
                       flush=True)
-            # reduced storage: FP32 (u, v, qdata) and BF16 (u, qdata; FP32 v), public applies
-            for name, uu, vv, ab in (
-                    ("fp32", u.float(), torch.empty(nc * N, dtype=torch.float32, device=dev),
-                     ne * (4 * Pp**dim + 4 * Qq**dim) + 8 * nc * N),
-                    ("bf16", u.to(torch.bfloat16), torch.empty(nc * N, dtype=torch.float32, device=dev),
-                     ne * (4 * Pp**dim + 2 * Qq**dim) + 6 * nc * N)):
-                fn = op.apply_f32 if name == "fp32" else op.apply_bf16
+            # reduced storage: FP32 (u, v, qdata) and BF16 (u, qdata; FP32 v), public applies;
+            # in 3D at P >= 6, Q <= 8 also the tensor-core forms (3xTF32, one TF32 part, BF16)
+            ab32 = ne * (4 * Pp**dim + 4 * Qq**dim) + 8 * nc * N
+            ab16 = ne * (4 * Pp**dim + 2 * Qq**dim) + 6 * nc * N
+            forms = [("fp32", "f32", op.apply_f32, ab32), ("bf16", "bf16", op.apply_bf16, ab16)]
+            if dim == 3 and 6 <= Pp <= 8 and Qq <= 8:
+                forms += [("fp32_tc_3xtf32", "f32", lambda a, b: op.apply_f32_tc(a, b, split=True), ab32),
+                          ("fp32_tc_tf32", "f32", lambda a, b: op.apply_f32_tc(a, b, split=False), ab32),
+                          ("bf16_tc", "bf16", op.apply_bf16_tc, ab16)]
+            for name, st, fn, ab in forms:
+                uu = u.float() if st == "f32" else u.to(torch.bfloat16)
+                vv = torch.empty(nc * N, dtype=torch.float32, device=dev)
                 for _ in range(3):
                     fn(uu, vv)
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -472,6 +477,10 @@ def run_sweep(args):
                                   "algorithmic_bytes": ab, "roofline_frac": ab / (ms * 1e-3) / 1e9 / peak}),
                       flush=True)
                 del uu, vv
+            if args.sweep_storage_only:
+                del op, ru, qd, u, v
+                torch.cuda.empty_cache()
+                continue
             op.set_kernel(fem.KernelVariant.auto)
             ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             ev[0].record()
@@ -982,6 +991,9 @@ def main():
     ap.add_argument("--sweep-P", default="2,3,4,5,6,7,8")
     ap.add_argument("--sweep-dim", default="3", help="dimensions of the order sweep, e.g. 2,3")
     ap.add_argument("--sweep-steps", type=int, default=20)
+    ap.add_argument("--sweep-dofs", type=int, default=64_000_000, help="DoFs of each sweep mesh")
+    ap.add_argument("--sweep-storage-only", action="store_true",
+                    help="sweep only the reduced-storage and tensor-core applies (no FP64 variants, no basis)")
     ap.add_argument("--solve", action="store_true", help="mixed-precision mass solve, FP64 vs FP32+IR (extra lines)")
     ap.add_argument("--solve-shape", default="64,64,64")
     ap.add_argument("--solve-P", type=int, default=5)

@@ -29,8 +29,9 @@
 // Padding: rows and K entries beyond an axis hold stale but finite values
 // from other stages (the buffers are zeroed once per CTA), and the B
 // operands are zero beyond the axes, so padding contributes exact zeros.
-// Persistent CTAs over tiles (round-robin), tensor memory allocated once per
-// CTA; every wait on the tensor cores is bounded (status bit 2 on timeout).
+// Persistent CTAs taking tiles from a ticket, tensor memory allocated once
+// per CTA; every wait on the tensor cores is bounded (status bit 2 on
+// timeout).
 #pragma once
 #include <cuda_runtime.h>
 
@@ -44,8 +45,9 @@ namespace fem_b200 {
 // The B operands of the six stages, as the 16 x 8 K-major shared-memory
 // image (tc::kmajor_index): forward [q][p] and backward [p][q], each as
 // {B_hi; B_lo} and {B_hi; 0}.
+constexpr int kTcOpFloats = 2 * tc::kTcSboBytes / 4;  // 16 rows: two row groups
 struct TcMats {
-  float op[4][128];  // 0 fwd split, 1 fwd hi, 2 bwd split, 3 bwd hi
+  float op[4][kTcOpFloats];  // 0 fwd split, 1 fwd hi, 2 bwd split, 3 bwd hi
 };
 
 template <int P, int Q>
@@ -55,13 +57,13 @@ struct TcMass3D {
   static constexpr int ES = P * P * P;
   static constexpr int G = P > Q ? P : Q;
   static constexpr int NBLK = (E * G * 8 + 127) / 128;  // M blocks of the widest stage (<= 4)
-  static constexpr int A_FLOATS = NBLK * 1024;          // one operand buffer: NBLK x 128 rows x 8
+  static constexpr int A_FLOATS = NBLK * tc::kTcBlockFloats;  // one operand buffer: NBLK x 128 rows x 8
   static constexpr int TMEM_COLS = NBLK * 16 <= 32 ? 32 : 64;
   // dynamic shared memory: the operand buffers and the B operands, padded so
   // that at most 512 / TMEM_COLS CTAs fit on an SM (tensor memory never runs
   // short, so no CTA waits in its allocation)
   static constexpr int smem(bool split) {
-    const int need = ((split ? 2 : 1) * A_FLOATS + 4 * 128) * 4;
+    const int need = ((split ? 2 : 1) * A_FLOATS + 4 * kTcOpFloats) * 4;
     const int cap = 512 / TMEM_COLS;  // CTAs a SM's tensor memory holds
     const int floor_bytes = 233472 / (cap + 1) + 1024;
     return need > floor_bytes ? need : floor_bytes;
@@ -74,20 +76,22 @@ __global__ void __launch_bounds__(128) mass3d_apply_tc_kernel(const __grid_const
                                                              const int* __restrict__ offs, const S* __restrict__ qd,
                                                              const S* __restrict__ u, float* __restrict__ v,
                                                              int num_elem, int num_comp_run, int64_t comp_stride,
-                                                             int64_t n_tiles, int* __restrict__ status) {
+                                                             int64_t n_tiles, int* __restrict__ ticket,
+                                                             int* __restrict__ status) {
   using L = TcMass3D<P, Q>;
   static_assert(P <= 8 && Q <= 8, "one K = 8 step a contraction");
   extern __shared__ __align__(1024) unsigned char tc_smem_bytes[];
   float* smem = reinterpret_cast<float*>(tc_smem_bytes);
   float* a_hi = smem;
   float* a_lo = smem + L::A_FLOATS;                       // SPLIT only
-  float* bops = smem + (SPLIT ? 2 : 1) * L::A_FLOATS;    // 4 x 128
+  float* bops = smem + (SPLIT ? 2 : 1) * L::A_FLOATS;    // 4 operands
   __shared__ __align__(8) uint64_t bar;
   __shared__ uint32_t taddr_s;
+  __shared__ int tile_s;
   const int tid = threadIdx.x, warp = tid >> 5;
 
   for (int i = tid; i < (SPLIT ? 2 : 1) * L::A_FLOATS; i += L::NT) smem[i] = 0.0f;
-  for (int i = tid; i < 4 * 128; i += L::NT) bops[i] = mats.op[i / 128][i % 128];
+  for (int i = tid; i < 4 * kTcOpFloats; i += L::NT) bops[i] = mats.op[i / kTcOpFloats][i % kTcOpFloats];
   if (tid == 0) tc::mbar_init(&bar, 1);
   if (warp == 0) tc::tmem_alloc(&taddr_s, L::TMEM_COLS);
   tc::fence_before_sync();
@@ -106,12 +110,15 @@ __global__ void __launch_bounds__(128) mass3d_apply_tc_kernel(const __grid_const
     __syncthreads();
     if (tid == 0) {
       tc::fence_after_sync();
-      const uint64_t b_split = tc::kmajor_desc(b_addr + uint32_t(bwd) * 1024);
-      const uint64_t b_hi = tc::kmajor_desc(b_addr + uint32_t(bwd) * 1024 + 512);
+      constexpr uint32_t op_bytes = kTcOpFloats * 4, blk_bytes = tc::kTcBlockFloats * 4;
+      const uint64_t b_split = tc::kmajor_desc(b_addr + uint32_t(bwd) * 2 * op_bytes);
+      const uint64_t b_hi = tc::kmajor_desc(b_addr + uint32_t(bwd) * 2 * op_bytes + op_bytes);
       for (int blk = 0; blk < nblk; ++blk) {
-        tc::mma_tf32(tmem + uint32_t(blk) * 16, tc::kmajor_desc(a_hi_addr + uint32_t(blk) * 4096), b_split, idesc, 0);
+        tc::mma_tf32(tmem + uint32_t(blk) * 16, tc::kmajor_desc(a_hi_addr + uint32_t(blk) * blk_bytes), b_split, idesc,
+                     0);
         if constexpr (SPLIT)
-          tc::mma_tf32(tmem + uint32_t(blk) * 16, tc::kmajor_desc(a_lo_addr + uint32_t(blk) * 4096), b_hi, idesc, 1);
+          tc::mma_tf32(tmem + uint32_t(blk) * 16, tc::kmajor_desc(a_lo_addr + uint32_t(blk) * blk_bytes), b_hi, idesc,
+                       1);
       }
       tc::mma_commit(&bar);
     }
@@ -128,29 +135,36 @@ __global__ void __launch_bounds__(128) mass3d_apply_tc_kernel(const __grid_const
     for (int j = 0; j < 8; ++j) d[j] = r[j] + r[j + 8];
   };
   auto put = [&](int R, int k, float x) {
-    const int idx = (R >> 7) * 1024 + tc::kmajor_index(R & 127, k);
+    const int idx = (R >> 7) * tc::kTcBlockFloats + tc::kmajor_index(R & 127, k);
     const float hi = tc::to_tf32(x);
     a_hi[idx] = hi;
     if constexpr (SPLIT) a_lo[idx] = tc::to_tf32(x - hi);
   };
   auto put_row = [&](int R, const float (&x)[8]) {
-    const int idx = (R >> 7) * 1024 + tc::kmajor_index(R & 127, 0);
+    const int idx = (R >> 7) * tc::kTcBlockFloats + tc::kmajor_index(R & 127, 0);
+    constexpr int K4 = tc::kTcLboBytes / 4;  // the second K half
     float h[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) h[k] = tc::to_tf32(x[k]);
     *reinterpret_cast<float4*>(a_hi + idx) = make_float4(h[0], h[1], h[2], h[3]);
-    *reinterpret_cast<float4*>(a_hi + idx + 32) = make_float4(h[4], h[5], h[6], h[7]);
+    *reinterpret_cast<float4*>(a_hi + idx + K4) = make_float4(h[4], h[5], h[6], h[7]);
     if constexpr (SPLIT) {
       float l[8];
 #pragma unroll
       for (int k = 0; k < 8; ++k) l[k] = tc::to_tf32(x[k] - h[k]);
       *reinterpret_cast<float4*>(a_lo + idx) = make_float4(l[0], l[1], l[2], l[3]);
-      *reinterpret_cast<float4*>(a_lo + idx + 32) = make_float4(l[4], l[5], l[6], l[7]);
+      *reinterpret_cast<float4*>(a_lo + idx + K4) = make_float4(l[4], l[5], l[6], l[7]);
     }
   };
   constexpr int NBP = L::nblk(P), NBQ = L::nblk(Q);
 
-  for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+  // tiles from a ticket (zeroed before the launch): a CTA that becomes
+  // resident late takes what is left, so the load stays balanced
+  for (;;) {
+    if (tid == 0) tile_s = atomicAdd(ticket, 1);
+    __syncthreads();
+    const int64_t tile = tile_s;
+    if (tile >= n_tiles) break;
     for (int comp = 0; comp < num_comp_run; ++comp) {
       const int64_t ks = comp * comp_stride;
       // S1: gather, rows (e,pz,py), K = px

@@ -254,6 +254,7 @@ struct MassPlan {
   DevBuf<float> qd_t32, dinv32, evec32;   // FP32 copies (inner solves, FP32 applies)
   DevBuf<__nv_bfloat16> qd_t16;           // BF16 qdata (BF16-storage applies)
   DevBuf<float> f_r, f_p, f_s, f_w, f_x;  // FP32 Krylov vectors
+  DevBuf<int> tc_ticket;                  // tile counter of the tensor-core apply (zeroed before each launch)
 };
 
 template <int P, int Q>

@@ -181,9 +181,16 @@ void launch_tc(const MassPlan& p, const S* qd, const S* u, float* v, cudaStream_
   const auto kern = mass3d_apply_tc_kernel<P, Q, SPLIT, S>;
   static std::atomic<uint64_t> smem_set{0};
   set_smem(kern, smem, smem_set);
-  const int grid = int(std::min<int64_t>(p.n_tiles, resident_ctas(reinterpret_cast<const void*>(kern), L::NT, smem)));
+  // persistent CTAs: 8 a SM (the shared-memory padding of TcMass3D::smem keeps
+  // at most as many resident as tensor memory holds), tiles from a ticket
+  int sms = 0;
+  FEM_CUDA_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p.device));
+  const int grid = int(std::min<int64_t>(p.n_tiles, int64_t(sms) * 8));
+  MassPlan& mp = const_cast<MassPlan&>(p);
+  if (!mp.tc_ticket.get()) mp.tc_ticket.alloc(1);
+  FEM_CUDA_CHECK(cudaMemsetAsync(mp.tc_ticket.get(), 0, sizeof(int), s));
   kern<<<grid, L::NT, smem, s>>>(tc_mats(p.basis), p.offs_t.get(), qd, u, v, p.num_elem, p.comp_run, p.comp_stride,
-                                 p.n_tiles, p.status.get());
+                                 p.n_tiles, mp.tc_ticket.get(), p.status.get());
   FEM_LAUNCH_CHECK();
 }
 

@@ -92,19 +92,26 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
 }
 
 // Canonical K-major layout without swizzle, for 32-bit elements: an operand
-// of R rows x 8 columns (one K = 8 MMA step), element (r, k) at byte
-//   (r % 8) * 16 + (r / 8) * 256 + (k / 4) * 128 + (k % 4) * 4,
-// i.e. 8-row x 16-byte core matrices, the two K halves 128 bytes apart
-// (leading byte offset) and row groups 256 bytes apart (stride byte offset).
-__host__ __device__ constexpr int kmajor_index(int r, int k) { return (r % 8) * 4 + (r / 8) * 64 + (k / 4) * 32 + k % 4; }
+// of R rows x 8 columns (one K = 8 MMA step) in 8-row x 16-byte core
+// matrices, element (r, k) at byte
+//   (r % 8) * 16 + (r / 8) * 288 + (k / 4) * 144 + (k % 4) * 4,
+// i.e. the two K halves 144 bytes apart (leading byte offset) and row groups
+// 288 bytes apart (stride byte offset).  The strides are padded past the
+// dense 128 / 256 so that the column-wise (transposing) stores of a warp --
+// 8 lanes a row group, 4 row groups -- fall in 32 distinct banks.
+constexpr int kTcLboBytes = 144, kTcSboBytes = 288;
+constexpr int kTcBlockFloats = 16 * kTcSboBytes / 4;  // 128 rows
+__host__ __device__ constexpr int kmajor_index(int r, int k) {
+  return (r % 8) * 4 + (r / 8) * (kTcSboBytes / 4) + (k / 4) * (kTcLboBytes / 4) + k % 4;
+}
 
 // Shared-memory matrix descriptor of that layout: start address, leading and
 // stride byte offsets (multiples of 16 bytes), version 1, no swizzle.
 __device__ __forceinline__ uint64_t kmajor_desc(uint32_t addr) {
   uint64_t d = 0;
   d |= uint64_t((addr >> 4) & 0x3FFF);
-  d |= uint64_t((128u >> 4) & 0x3FFF) << 16;
-  d |= uint64_t((256u >> 4) & 0x3FFF) << 32;
+  d |= uint64_t((uint32_t(kTcLboBytes) >> 4) & 0x3FFF) << 16;
+  d |= uint64_t((uint32_t(kTcSboBytes) >> 4) & 0x3FFF) << 32;
   d |= uint64_t(1) << 46;  // version (sm_100); base offset 0, layout type 0 (no swizzle)
   return d;
 }

@@ -19,8 +19,8 @@ namespace {
 // tensor memory (thread t: row t).  A [128][8], B [16][8], D [128][16].
 __global__ void __launch_bounds__(128) tc_selftest_kernel(const float* __restrict__ A, const float* __restrict__ B,
                                                           float* __restrict__ D, int* __restrict__ status) {
-  __shared__ __align__(1024) float a_k[128 * 8];
-  __shared__ __align__(1024) float b_k[16 * 8];
+  __shared__ __align__(1024) float a_k[tc::kTcBlockFloats];
+  __shared__ __align__(1024) float b_k[2 * tc::kTcSboBytes / 4];
   __shared__ __align__(8) uint64_t bar;
   __shared__ uint32_t taddr_s;
   const int t = threadIdx.x, warp = t >> 5;
