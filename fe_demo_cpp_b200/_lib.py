@@ -74,6 +74,8 @@ SIGNATURES = {
     "fem_b200_batch_bind": ([_p, _p, _p, _p], _i),
     "fem_b200_batch_apply": ([_p, _i, _p], _i),
     "fem_b200_batch_autotune": ([_p, _i, _p], _i),
+    "fem_b200_batch_set_mode": ([_p, _i], _i),
+    "fem_b200_batch_check": ([_p, _p], _i),
     "fem_b200_batch_info": ([_p, _p, _p, _p, _p, _p, _p], _i),
     "fem_b200_batch_destroy": ([_p], _i),
     "fem_b200_server_create": ([_i, _i64, _p], _i),

@@ -401,6 +401,17 @@ class Batch(_Handle):
     def autotune(self, reps=5, stream=None) -> None:
         call("fem_b200_batch_autotune", self.h, int(reps), _stream(stream))
 
+    MODES = {"auto": 0, "classes": 1, "persistent": 2}
+
+    def set_mode(self, mode: str) -> None:
+        """'persistent': one kernel launch for the whole batch; 'classes': one
+        kernel per class; 'auto': the former where it applies, unless
+        autotuning found the latter faster."""
+        call("fem_b200_batch_set_mode", self.h, self.MODES[mode])
+
+    def check(self, stream=None) -> None:
+        call("fem_b200_batch_check", self.h, _stream(stream))
+
     def info(self) -> dict:
         nc, gk, pc, br = C.c_int(0), C.c_int(0), C.c_int(0), C.c_int(0)
         tiles, dofs = C.c_int64(0), C.c_int64(0)

@@ -131,6 +131,156 @@ __global__ void __launch_bounds__(128)
 }
 
 // ---------------------------------------------------------------------------
+// One persistent launch for the whole batch.  Work items come from a ticket:
+// first the zeroing of every v_i in chunks, then, class by class (heaviest
+// first), groups of tiles of one mesh.  The block has kPersistBD threads and
+// runs K = kPersistBD / NT tiles of a class at once in thread groups of the
+// class's tile width NT (a P = 2 3D tile needs 72 threads, a P = 6 one 392),
+// each group with its own slice of shared memory; threads beyond K * NT only
+// join the barriers.  The shapes compiled in are those of uneven mesh
+// batches: dim 2 and 3, P = 2..6, Q = P + 1, one basis a P (the Lagrange
+// basis on GLL nodes at Gauss points; the 1D matrices travel in the kernel
+// parameter).  Compute items wait (bounded) until every zeroing item is
+// done -- once a block, the counter is then known complete; zeroing items
+// come first in ticket order and wait on nothing, so the wait ends.
+// ---------------------------------------------------------------------------
+constexpr int kPersistBD = 416;          // 13 warps: the 3D P = 6 tile (392 threads), rounded up
+constexpr int kPersistZeroChunk = 1 << 16;  // entries of v a zeroing item
+
+template <class T>
+struct PersistMats {
+  Mat1D<2, 3, T> p2;
+  Mat1D<3, 4, T> p3;
+  Mat1D<4, 5, T> p4;
+  Mat1D<5, 6, T> p5;
+  Mat1D<6, 7, T> p6;
+};
+
+template <int P, class T>
+__device__ __forceinline__ const Mat1D<P, P + 1, T>& persist_mat(const PersistMats<T>& m) {
+  if constexpr (P == 2) return m.p2;
+  else if constexpr (P == 3) return m.p3;
+  else if constexpr (P == 4) return m.p4;
+  else if constexpr (P == 5) return m.p5;
+  else return m.p6;
+}
+
+// the even-odd contractions where the class kernels use them (centro-symmetric
+// bases only: the plan checks)
+template <int P, class T>
+constexpr bool persist_even_odd() {
+  return sizeof(T) == 8 ? (P == 4 || P == 6) : P == 6;
+}
+
+template <int D, int P>
+struct PersistShape {
+  static constexpr int Q = P + 1;
+  static constexpr int NT = D == 3 ? Mass3D<P, Q>::NT : Mass2D<P, Q>::NT;
+  static constexpr int K = kPersistBD / NT;  // tiles a block runs at once
+  template <class T>
+  static constexpr int smem() {
+    return D == 3 ? (Mass3D<P, Q>::SA + Mass3D<P, Q>::SB) * int(sizeof(T)) : (Mass2D<P, Q>::S1 + Mass2D<P, Q>::S3) * int(sizeof(T));
+  }
+  static constexpr int slot = (D - 2) * 5 + (P - 2);  // the class id in the work items
+};
+
+template <class T>
+constexpr int persist_smem() {
+  int m = 0;
+#define FEM_PERSIST_MAX(D, P) m = cmax(m, PersistShape<D, P>::K * PersistShape<D, P>::template smem<T>());
+  FEM_PERSIST_MAX(2, 2) FEM_PERSIST_MAX(2, 3) FEM_PERSIST_MAX(2, 4) FEM_PERSIST_MAX(2, 5) FEM_PERSIST_MAX(2, 6)
+  FEM_PERSIST_MAX(3, 2) FEM_PERSIST_MAX(3, 3) FEM_PERSIST_MAX(3, 4) FEM_PERSIST_MAX(3, 5) FEM_PERSIST_MAX(3, 6)
+#undef FEM_PERSIST_MAX
+  return m;
+}
+
+// Up to K tiles (tile0 ..) of one mesh, one a thread group.
+template <int D, int P, class T>
+__device__ __forceinline__ void persist_tiles(const PersistMats<T>& mats, const BatchMesh<T>& mm, int tile0,
+                                              int count, unsigned char* smem) {
+  using S = PersistShape<D, P>;
+  constexpr int Q = S::Q;
+  const int g = int(threadIdx.x) / S::NT;
+  const bool in_group = g < min(S::K, count);
+  const int t = in_group ? int(threadIdx.x) % S::NT : S::NT;
+  T* base = reinterpret_cast<T*>(smem + (in_group ? g : 0) * S::template smem<T>());
+  double dsum = 0.0;
+  const int64_t tile = tile0 + (in_group ? g : 0);
+  if constexpr (D == 3) {
+    using L = Mass3D<P, Q>;
+    mass3d_tile<P, Q, T, ApplyPlain, 1, T, Mat1D<P, Q, T>, persist_even_odd<P, T>()>(
+        persist_mat<P>(mats), base, base + L::SA, mm.offs, mm.qd, mm.u, mm.v, nullptr, mm.num_elem, mm.comp_run,
+        mm.comp_stride, ApplyPlain{}, tile, dsum, t);
+  } else {
+    using L = Mass2D<P, Q>;
+    mass2d_tile<P, Q, T, ApplyPlain, T, Mat1D<P, Q, T>, false>(persist_mat<P>(mats), base, base + L::S1, mm.offs,
+                                                               mm.qd, mm.u, mm.v, nullptr, mm.num_elem, mm.comp_run,
+                                                               mm.comp_stride, ApplyPlain{}, tile, dsum, t);
+  }
+}
+
+// items[i] = {class slot (-1: zero a chunk of v), mesh, first tile (or chunk), tile count};
+// ctl[0] the ticket, ctl[1] zeroing items done (both zeroed before the launch)
+template <class T, int MINB>
+__global__ void __launch_bounds__(kPersistBD, MINB)
+    batch_persistent_kernel(const __grid_constant__ PersistMats<T> mats, const BatchMesh<T>* __restrict__ meshes,
+                            const int4* __restrict__ items, int n_items, int n_zero_items, int* __restrict__ ctl,
+                            int* __restrict__ status) {
+  extern __shared__ __align__(16) unsigned char smem_bytes[];
+  __shared__ int s_item;
+  bool ready = false;  // every thread alike: the zeroing is known complete
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(ctl, 1);
+    __syncthreads();
+    const int it = s_item;
+    if (it >= n_items) break;
+    const int4 w = items[it];
+    const BatchMesh<T> mm = meshes[w.y];
+    if (w.x < 0) {
+      const int64_t a = int64_t(w.z) * kPersistZeroChunk;
+      const int64_t b = min(mm.l_size, a + kPersistZeroChunk);
+      for (int64_t i = a + threadIdx.x; i < b; i += blockDim.x) mm.v[i] = T(0);
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(ctl + 1, 1);
+      }
+      continue;
+    }
+    if (!ready) {
+      if (threadIdx.x == 0) {
+        int spins = 0;
+        while (true) {
+          int done;
+          asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(done) : "l"(ctl + 1) : "memory");
+          if (done >= n_zero_items) break;
+          if (++spins > (1 << 22)) {
+            atomicOr(status, 8);
+            break;
+          }
+          __nanosleep(100);
+        }
+      }
+      __syncthreads();
+      ready = true;
+    }
+    switch (w.x) {
+      case PersistShape<2, 2>::slot: persist_tiles<2, 2, T>(mats, mm, w.z, w.w, smem_bytes); break;
+      case PersistShape<2, 3>::slot: persist_tiles<2, 3, T>(mats, mm, w.z, w.w, smem_bytes); break;
+      case PersistShape<2, 4>::slot: persist_tiles<2, 4, T>(mats, mm, w.z, w.w, smem_bytes); break;
+      case PersistShape<2, 5>::slot: persist_tiles<2, 5, T>(mats, mm, w.z, w.w, smem_bytes); break;
+      case PersistShape<2, 6>::slot: persist_tiles<2, 6, T>(mats, mm, w.z, w.w, smem_bytes); break;
+      case PersistShape<3, 2>::slot: persist_tiles<3, 2, T>(mats, mm, w.z, w.w, smem_bytes); break;
+      case PersistShape<3, 3>::slot: persist_tiles<3, 3, T>(mats, mm, w.z, w.w, smem_bytes); break;
+      case PersistShape<3, 4>::slot: persist_tiles<3, 4, T>(mats, mm, w.z, w.w, smem_bytes); break;
+      case PersistShape<3, 5>::slot: persist_tiles<3, 5, T>(mats, mm, w.z, w.w, smem_bytes); break;
+      default: persist_tiles<3, 6, T>(mats, mm, w.z, w.w, smem_bytes); break;
+    }
+    __syncthreads();  // the groups' shared memory and s_item are reused by the next item
+  }
+}
+
+// ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
 template <int P, int Q, class T>
@@ -275,6 +425,20 @@ struct BatchPlan {
   cudaGraphExec_t exec = nullptr;
   int graph_kernels = 0;
   int branches = 1;  // parallel graph branches (classes run concurrently), autotuned
+  // the one-launch form (batch_persistent_kernel): eligible when every class
+  // is one of its compiled shapes; mode FEM_B200_BATCH_AUTO runs it unless
+  // the autotuner found the per-class graph faster
+  bool persist_ok = false;
+  int mode = FEM_B200_BATCH_AUTO;
+  bool persist_chosen = true;  // AUTO's choice
+  DevBuf<int4> items;
+  int n_items = 0, n_zero_items = 0;
+  DevBuf<int> ctl;     // ticket, zeroing items done
+  DevBuf<int> status;  // bit 3: the wait for the zeroing ran out
+  std::vector<unsigned char> persist_mats;  // PersistMats<T>, the kernel parameter
+  bool persistent() const {
+    return persist_ok && (mode == FEM_B200_BATCH_PERSISTENT || (mode == FEM_B200_BATCH_AUTO && persist_chosen));
+  }
 
   ~BatchPlan() {
     int prev = -1;
@@ -297,9 +461,91 @@ struct BatchPlan {
   }
 };
 
+template <class T, int MINB>
+void launch_persistent(BatchPlan& b, cudaStream_t s) {
+  constexpr int smem = persist_smem<T>();
+  const auto kern = batch_persistent_kernel<T, MINB>;
+  static std::atomic<uint64_t> smem_set{0};
+  set_smem(kern, smem, smem_set);
+  const int grid = int(std::min<int64_t>(b.n_items, resident_ctas(reinterpret_cast<const void*>(kern), kPersistBD, smem)));
+  FEM_CUDA_CHECK(cudaMemsetAsync(b.ctl.get(), 0, 2 * sizeof(int), s));
+  PersistMats<T> m;
+  std::memcpy(&m, b.persist_mats.data(), sizeof(m));
+  kern<<<grid, kPersistBD, smem, s>>>(m, reinterpret_cast<const BatchMesh<T>*>(b.meshes.get()), b.items.get(),
+                                      b.n_items, b.n_zero_items, b.ctl.get(), b.status.get());
+  FEM_LAUNCH_CHECK();
+}
+
+template <class T>
+void fill_persist_mats(BatchPlan& b) {
+  PersistMats<T> m;
+  std::memset(&m, 0, sizeof(m));
+  for (const BatchClass& c : b.classes) {
+    switch (c.P) {
+      case 2: m.p2 = batch_mat<2, 3, T>(c.basis); break;
+      case 3: m.p3 = batch_mat<3, 4, T>(c.basis); break;
+      case 4: m.p4 = batch_mat<4, 5, T>(c.basis); break;
+      case 5: m.p5 = batch_mat<5, 6, T>(c.basis); break;
+      default: m.p6 = batch_mat<6, 7, T>(c.basis); break;
+    }
+  }
+  b.persist_mats.resize(sizeof(m));
+  std::memcpy(b.persist_mats.data(), &m, sizeof(m));
+}
+
+// The work items of the one-launch form, when every class fits it: dim 2 or
+// 3, P = 2..6, Q = P + 1, one 1D matrix a P, centro-symmetric where the
+// kernel takes the even-odd contractions.
+void plan_persistent(BatchPlan& b) {
+  const bool fp32 = b.precision == FEM_B200_PRECISION_FP32;
+  std::map<int, std::vector<double>> interp_of_p;
+  for (const BatchClass& c : b.classes) {
+    if (c.dim < 2 || c.P < 2 || c.P > 6 || c.Q != c.P + 1) return;
+    const bool eo = fp32 ? c.P == 6 : (c.P == 4 || c.P == 6);
+    if (eo && !c.centro_symmetric) return;
+    auto it = interp_of_p.find(c.P);
+    if (it != interp_of_p.end() && it->second != c.basis.interp) return;
+    interp_of_p[c.P] = c.basis.interp;
+  }
+  std::vector<int4> items;
+  for (size_t i = 0; i < b.ops.size(); ++i) {
+    const int64_t chunks = (b.ops[i]->l_size + kPersistZeroChunk - 1) / kPersistZeroChunk;
+    for (int64_t k = 0; k < chunks; ++k) items.push_back(make_int4(-1, int(i), int(k), 0));
+  }
+  const int n_zero = int(items.size());
+  for (const BatchClass& c : b.classes) {  // heaviest first (the classes' order)
+    const int slot = (c.dim - 2) * 5 + (c.P - 2);
+    const int nt = c.dim == 3 ? 8 * c.Q * c.Q : 32 * c.Q;
+    const int k = kPersistBD / nt;
+    for (int i : c.members)
+      for (int64_t t = 0; t < b.ops[size_t(i)]->n_tiles; t += k)
+        items.push_back(make_int4(slot, i, int(t), int(std::min<int64_t>(k, b.ops[size_t(i)]->n_tiles - t))));
+  }
+  if (items.size() >= size_t(INT32_MAX)) return;
+  b.items.alloc(items.size());
+  FEM_CUDA_CHECK(cudaMemcpy(b.items.get(), items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice));
+  b.n_items = int(items.size());
+  b.n_zero_items = n_zero;
+  b.ctl.alloc(2);
+  b.status.alloc(1);
+  FEM_CUDA_CHECK(cudaMemset(b.status.get(), 0, sizeof(int)));
+  if (fp32)
+    fill_persist_mats<float>(b);
+  else
+    fill_persist_mats<double>(b);
+  b.persist_ok = true;
+}
+
 // Every v_i zeroed, then every class (the heaviest first, round-robin over
-// `branches` streams, which fork from and join into s0).
+// `branches` streams, which fork from and join into s0); or the one launch.
 void enqueue_batch(BatchPlan& b, cudaStream_t s0, int branches) {
+  if (b.persistent()) {
+    if (b.precision == FEM_B200_PRECISION_FP32)
+      launch_persistent<float, 3>(b, s0);
+    else
+      launch_persistent<double, 2>(b, s0);
+    return;
+  }
   const unsigned ops = unsigned(b.ops.size());
   const unsigned zx = unsigned(std::max<int64_t>(1, std::min<int64_t>(64, (b.max_l_size + 2047) / 2048)));
   if (b.precision == FEM_B200_PRECISION_FP32)
@@ -341,7 +587,7 @@ void capture_batch(BatchPlan& b) {
   }
   FEM_CUDA_CHECK(cudaStreamEndCapture(s0, &b.graph));
   FEM_CUDA_CHECK(cudaGraphInstantiate(&b.exec, b.graph, 0));
-  b.graph_kernels = 1 + int(b.classes.size());
+  b.graph_kernels = b.persistent() ? 1 : 1 + int(b.classes.size());
 }
 
 // Two timing events (RAII); time(s, f) = device ms of what f enqueues in s.
@@ -457,6 +703,7 @@ int fem_b200_batch_create(const fem_b200_mass* ops, int num_ops, int precision, 
     // heaviest classes first, so the parallel branches start with the long kernels
     std::stable_sort(b->classes.begin(), b->classes.end(),
                      [](const BatchClass& x, const BatchClass& y) { return x.n_tiles > y.n_tiles; });
+    plan_persistent(*b);
     b->meshes.alloc(b->ops.size() * b->mesh_bytes());
     for (auto& st : b->streams) FEM_CUDA_CHECK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     FEM_CUDA_CHECK(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
@@ -531,6 +778,7 @@ int fem_b200_batch_autotune(fem_b200_batch batch, int reps, void* stream) {
     // contend for HBM, which pays off in some precisions only
     float best = 0.0f;
     int best_branches = 1;
+    b.persist_chosen = false;  // the per-class graph first
     for (int nb : {1, 2, 4}) {
       b.branches = nb;
       capture_batch(b);
@@ -541,9 +789,51 @@ int fem_b200_batch_autotune(fem_b200_batch batch, int reps, void* stream) {
       if (nb == 1 || ms < best) best = ms, best_branches = nb;
     }
     b.branches = best_branches;
+    // then the one persistent launch against that graph of class kernels
+    if (b.persist_ok && b.mode == FEM_B200_BATCH_AUTO) {
+      b.persist_chosen = true;
+      capture_batch(b);
+      FEM_CUDA_CHECK(cudaGraphLaunch(b.exec, s));  // warm-up
+      const float ms = ev.time(s, [&] {
+        for (int r = 0; r < reps; ++r) FEM_CUDA_CHECK(cudaGraphLaunch(b.exec, s));
+      });
+      b.persist_chosen = ms <= best;
+    }
     capture_batch(b);
     FEM_CUDA_CHECK(cudaGraphLaunch(b.exec, s));  // leaves v_i = M_i u_i
     FEM_CUDA_CHECK(cudaStreamSynchronize(s));
+  });
+}
+
+int fem_b200_batch_set_mode(fem_b200_batch batch, int mode) {
+  return guarded([&] {
+    require(batch && batch->d, "batch mode: NULL handle");
+    BatchPlan& b = *batch->d;
+    require(mode == FEM_B200_BATCH_AUTO || mode == FEM_B200_BATCH_CLASSES || mode == FEM_B200_BATCH_PERSISTENT,
+            "batch mode: unknown mode");
+    if (mode == FEM_B200_BATCH_PERSISTENT && !b.persist_ok)
+      throw unsupported_error("batch mode: the one-launch kernel covers dim 2 and 3, P = 2..6, Q = P + 1 with one "
+                              "basis a P; this batch has other classes");
+    DeviceGuard g(b.device);
+    b.mode = mode;
+    b.drop_graph();
+  });
+}
+
+int fem_b200_batch_check(fem_b200_batch batch, void* stream) {
+  return guarded([&] {
+    require(batch && batch->d, "batch check: NULL handle");
+    BatchPlan& b = *batch->d;
+    DeviceGuard g(b.device);
+    FEM_CUDA_CHECK(cudaStreamSynchronize(as_stream(stream)));
+    if (!b.status.get()) return;
+    int st = 0;
+    FEM_CUDA_CHECK(cudaMemcpy(&st, b.status.get(), sizeof(int), cudaMemcpyDeviceToHost));
+    if (st) {
+      FEM_CUDA_CHECK(cudaMemset(b.status.get(), 0, sizeof(int)));
+      throw cuda_error("batch apply: a bounded wait in the persistent kernel ran out (status " + std::to_string(st) +
+                       "); the result is not valid");
+    }
   });
 }
 
@@ -558,7 +848,7 @@ int fem_b200_batch_info(fem_b200_batch batch, int* num_classes, int64_t* total_t
     if (num_classes) *num_classes = int(b.classes.size());
     if (total_tiles) *total_tiles = tiles;
     if (total_dofs) *total_dofs = dofs;
-    if (graph_kernels) *graph_kernels = 1 + int(b.classes.size());
+    if (graph_kernels) *graph_kernels = b.persistent() ? 1 : 1 + int(b.classes.size());
     if (persistent_classes) *persistent_classes = pers;
     if (graph_branches) *graph_branches = b.branches;
   });

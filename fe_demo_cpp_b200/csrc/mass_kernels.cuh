@@ -223,17 +223,21 @@ __device__ __forceinline__ void mass3d_tile(const M& m, T* __restrict__ sa, T* _
                                             const int* __restrict__ offs, const S* __restrict__ qd,
                                             const S* __restrict__ u, T* __restrict__ v, T* __restrict__ ev,
                                             int num_elem, int num_comp_run, int64_t comp_stride,
-                                            const Ext& ext, const int64_t tile, double& dsum) {
+                                            const Ext& ext, const int64_t tile, double& dsum, int t_in = -1) {
   using L = Mass3D<P, Q>;
   constexpr int E = L::E;
-  const int t = threadIdx.x, e = t % E, col = t / E;
+  // t_in: the thread's index in a group of L::NT running this tile (a block
+  // may run several tiles, or have threads to spare: t_in >= L::NT only
+  // takes part in the barriers)
+  const int t = t_in < 0 ? int(threadIdx.x) : t_in, e = t % E, col = t / E;
+  const bool live = t < L::NT;
   const bool nodal = col < P * P;  // (px, py) = (col % P, col / P)
   const bool mixed = col < P * Q;  // (px, qz) = (col % P, col / P)
   const int64_t eg = tile * E + e;
   const bool valid = eg < num_elem;
   // Prefetch: this thread's qdata row (qy, qz) = (col % Q, col / Q), all qx.
   T qv[Q];
-  {
+  if (live) {
     const S* qt = qd + tile * (int64_t(L::NQ) * E) + col * E + e;
 #pragma unroll
     for (int qx = 0; qx < Q; ++qx) qv[qx] = load_as<T>(qt + qx * (Q * Q * E));
@@ -303,7 +307,7 @@ __device__ __forceinline__ void mass3d_tile(const M& m, T* __restrict__ sa, T* _
       }
     }
     __syncthreads();
-    {  // phase C: x, pointwise mass, x^T
+    if (live) {  // phase C: x, pointwise mass, x^T
       const int qy = col % Q, qz = col / Q;
 #pragma unroll
       for (int c = 0; c < NCB; ++c) {
@@ -615,15 +619,17 @@ __device__ __forceinline__ void mass2d_tile(const M& m, T* __restrict__ s1, T* _
                                             const int* __restrict__ offs, const S* __restrict__ qd,
                                             const S* __restrict__ u, T* __restrict__ v, T* __restrict__ ev,
                                             int num_elem, int num_comp_run, int64_t comp_stride,
-                                            const Ext& ext, const int64_t tile, double& dsum) {
+                                            const Ext& ext, const int64_t tile, double& dsum, int t_in = -1) {
   using L = Mass2D<P, Q>;
   constexpr int E = L::E;
-  const int t = threadIdx.x, e = t % E, col = t / E;
+  // t_in: as mass3d_tile's (t_in >= L::NT: barriers only)
+  const int t = t_in < 0 ? int(threadIdx.x) : t_in, e = t % E, col = t / E;
+  const bool live = t < L::NT;
   const bool nodal = col < P;
   const int64_t eg = tile * E + e;
   const bool valid = eg < num_elem;
   T qv[Q];
-  {
+  if (live) {
     const S* qt = qd + tile * (int64_t(L::NQ) * E) + col * E + e;
 #pragma unroll
     for (int qx = 0; qx < Q; ++qx) qv[qx] = load_as<T>(qt + qx * (Q * E));
@@ -659,7 +665,7 @@ __device__ __forceinline__ void mass2d_tile(const M& m, T* __restrict__ s1, T* _
       }
     }
     __syncthreads();
-    {
+    if (live) {
       T w[P];
 #pragma unroll
       for (int px = 0; px < P; ++px) w[px] = s1[(px * Q + col) * E + e];

@@ -352,10 +352,19 @@ int fem_b200_mass_solve(fem_b200_mass op, const double *f, int64_t n_f, double *
 
 /* ---- batched apply over many meshes (no reference counterpart) ------------
  * One batch = many mass operators (any dim, P, Q, num_comp; atomic scatter)
- * applied together: v_i = M_i u_i for all i, as ONE captured CUDA graph
- * (a kernel zeroing every v_i, then one kernel per class of equal dim, P, Q,
- * components and basis over a device table of (mesh, tile) pairs, classes on
- * parallel graph branches).  The operators must outlive the batch.
+ * applied together: v_i = M_i u_i for all i, as ONE captured CUDA graph.
+ * Two forms: the one-launch form -- a single persistent kernel taking work
+ * items from a ticket: the zeroing of every v_i, then the tiles of every
+ * class, heaviest first, several low-order tiles a block at once; it covers
+ * dim 2 and 3, P = 2..6, Q = P + 1 with one basis a P -- and the per-class
+ * form (a kernel zeroing every v_i, then one kernel per class of equal dim,
+ * P, Q, components and basis over a device table of (mesh, tile) pairs,
+ * classes on parallel graph branches).  The operators must outlive the
+ * batch. */
+#define FEM_B200_BATCH_AUTO 0       /* the one-launch form where it applies, unless autotuning preferred the other */
+#define FEM_B200_BATCH_CLASSES 1    /* one kernel per class */
+#define FEM_B200_BATCH_PERSISTENT 2 /* one persistent launch (FEM_B200_ERROR_UNSUPPORTED where it does not apply) */
+/* Precision and layout as below.
  * Precision FEM_B200_PRECISION_FP32 applies FP32 u_i / v_i with FP32 qdata
  * (converted once from each operator's FP64 qdata). */
 #define FEM_B200_PRECISION_FP64 0
@@ -372,9 +381,15 @@ int fem_b200_batch_bind(fem_b200_batch b, const void *const *u, void *const *v, 
 int fem_b200_batch_apply(fem_b200_batch b, int use_graph, void *stream);
 /* Time each class's schedules (one CTA per tile; a persistent grid of
  * resident CTAs) over `reps` launches and keep the faster; then time the
- * graph with 1, 2 and 4 parallel branches and keep the fastest capture.
- * Leaves v_i = M_i u_i.  Synchronises the stream. */
+ * graph with 1, 2 and 4 parallel branches and keep the fastest capture; in
+ * mode FEM_B200_BATCH_AUTO also the one-launch form against that graph, and
+ * keep the faster.  Leaves v_i = M_i u_i.  Synchronises the stream. */
 int fem_b200_batch_autotune(fem_b200_batch b, int reps, void *stream);
+/* Choose the batch's form (FEM_B200_BATCH_*); drops the captured graph. */
+int fem_b200_batch_set_mode(fem_b200_batch b, int mode);
+/* Synchronise `stream` and report a bounded wait of the one-launch kernel
+ * that ran out as FEM_B200_ERROR_CUDA. */
+int fem_b200_batch_check(fem_b200_batch b, void *stream);
 /* Any output may be NULL: classes, tiles, sum of l_size (DoFs), kernels per
  * graph launch, classes on the persistent schedule, parallel graph branches. */
 int fem_b200_batch_info(fem_b200_batch b, int *num_classes, int64_t *total_tiles, int64_t *total_dofs,

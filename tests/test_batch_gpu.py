@@ -172,3 +172,74 @@ def test_batch_argument_errors(fem, cuda):
                            qd)
     with pytest.raises(fem.FemUnsupported):
         fem.Batch([ops[0], det], "fp64")
+
+
+def uneven_batch(fem, cuda, n=24, seed=3):
+    """Members of the uneven-mesh workload's family: 2D and 3D boxes, P 2..6,
+    Q = P + 1, 1-3 components (vector mass and the component-0-only
+    apply_mass), blocked and interleaved layouts, sizes from one element up."""
+    V, S = fem.QF.apply_mass_vector, fem.QF.apply_mass
+    rng = np.random.default_rng(seed)
+    ops, metas = [], []
+    for i in range(n):
+        dim = 2 + i % 2
+        P = 2 + (i // 2) % 5
+        nc = 1 + (i // 3) % 3
+        shape = tuple(int(x) for x in rng.integers(1, 6 if dim == 3 else 12, size=dim))
+        op, meta = make_op(fem, cuda, dim, shape, P, P + 1, nc, V if i % 4 else S, seed=100 + i,
+                           interleaved=(i % 5 == 1 and nc > 1))
+        ops.append(op)
+        metas.append(meta)
+    return ops, metas
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_persistent_batch_one_launch(fem, cuda, orc, precision):
+    """The whole batch in ONE persistent kernel launch: against each operator's
+    own apply (FP64: 1e-13; FP32: against the FP64 apply of the FP32-rounded
+    input, 1e-5), against the oracle on members of both dims, in both forms,
+    over repeated launches (the ticket is re-armed every time)."""
+    import torch
+    ops, metas = uneven_batch(fem, cuda)
+    dt = torch.float64 if precision == "fp64" else torch.float32
+    us = [dev(random_vector(mt["l_size"], 200 + i), cuda, dt) for i, mt in enumerate(metas)]
+    vs = [torch.full_like(u, float("nan")) for u in us]
+    b = fem.Batch(ops, precision)
+    b.bind(us, vs)
+    b.set_mode("persistent")
+    assert b.info()["graph_kernels"] == 1
+    tol = TOL if precision == "fp64" else 1e-5
+    for graph in (True, False, True):
+        for v in vs:
+            v.fill_(float("nan"))
+        b.apply(graph=graph)
+        b.check()
+        for i, op in enumerate(ops):
+            want = torch.empty(metas[i]["l_size"], dtype=torch.float64, device=cuda)
+            op.apply(us[i].double(), want)
+            close(host(vs[i]), host(want), tol)
+    for i in (0, 1, 7, 10):
+        mt = metas[i]
+        want = orc.mass_apply(mt["dim"], mt["ne"], mt["P"], mt["Q"], mt["nc"], mt["cs"], mt["l_size"], mt["offs"],
+                              mt["qd"], host(us[i]), vector=mt["vector"])
+        close(host(vs[i]), want, tol)
+    # the per-class form gives the same results; auto picks one after autotuning
+    first = [host(v) for v in vs]
+    b.set_mode("classes")
+    assert b.info()["graph_kernels"] == b.info()["classes"] + 1
+    b.apply()
+    for f, v in zip(first, vs):
+        close(host(v), f, tol)
+    b.set_mode("auto")
+    b.autotune(reps=2)
+    b.apply()
+    b.check()
+    for f, v in zip(first, vs):
+        close(host(v), f, tol)
+
+
+def test_persistent_batch_refuses_other_shapes(fem, cuda):
+    ops, metas = mixed_batch(fem, cuda)  # 1D members, Q != P + 1, P = 7, 8
+    b = fem.Batch(ops, "fp64")
+    with pytest.raises(fem.FemUnsupported):
+        b.set_mode("persistent")
