@@ -707,12 +707,24 @@ def run_batch(args):
         vv = [torch.empty_like(u) for u in uu]
         b = fem.Batch(ops, prec)
         b.bind(uu, vv)
-        results.append((prec, "batch, kernels launched directly", timed(lambda: b.apply(graph=False), K), b.info()))
-        results.append((prec, "batch, one graph launch", timed(lambda: b.apply(graph=True), K), b.info()))
-        b.autotune(reps=3)
-        results.append((prec, "batch, kernels launched directly, autotuned", timed(lambda: b.apply(graph=False), K),
+        # the per-class form: a zeroing kernel and one kernel per class
+        b.set_mode("classes")
+        results.append((prec, "per-class kernels launched directly", timed(lambda: b.apply(graph=False), K),
                         b.info()))
-        results.append((prec, "batch, one graph launch, autotuned", timed(lambda: b.apply(graph=True), K), b.info()))
+        b.autotune(reps=3)
+        results.append((prec, "per-class kernels, one graph launch, autotuned", timed(lambda: b.apply(graph=True), K),
+                        b.info()))
+        # the one-launch form: a single persistent kernel for the whole batch
+        b.set_mode("persistent")
+        results.append((prec, "one persistent kernel launch", timed(lambda: b.apply(graph=False), K), b.info()))
+        results.append((prec, "one persistent kernel launch, in a graph", timed(lambda: b.apply(graph=True), K),
+                        b.info()))
+        b.check()
+        # auto: the faster of the two after autotuning
+        b.set_mode("auto")
+        b.autotune(reps=3)
+        results.append((prec, "auto (autotuned choice), one graph launch", timed(lambda: b.apply(graph=True), K),
+                        b.info()))
         if prec == "fp64":
             # parity guard: the batch result against each operator's own apply
             worst = 0.0
@@ -890,6 +902,102 @@ def run_restriction(args):
 # end-to-end (host vectors) apply: the PCIe ceilings and the copy pipeline's
 # chunk count, on the bench workload (extra lines)
 # ---------------------------------------------------------------------------
+# ---------------------------------------------------------------------------
+# one mesh over the ranks (--split): the 100^3 P=5 mesh split into contiguous
+# element ranges (fem_b200_shard_*), each rank applying its elements, then one
+# interface exchange per apply: device pack, NCCL send/recv of the shared
+# values only, rank-ordered unpack-add (extra line; strong scaling: the mesh
+# is fixed as N grows)
+# ---------------------------------------------------------------------------
+def run_split(args, rank, world, local_rank):
+    import torch
+    import fe_demo_cpp_b200 as fem
+    from fe_demo_cpp_b200.build import build
+    from fe_demo_cpp_b200.mesh import box_mesh
+
+    build()
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    mesh = box_mesh(SHAPE, P, seed=SEED)
+    N = mesh.num_nodes
+    plan = fem.ShardPlan(mesh.offsets, P**3, world, rank)
+    n = plan.num_nodes
+    coords = np.concatenate([mesh.coords[k * N + plan.l2g] for k in range(3)])
+    rx = fem.Restriction(plan.num_elem, P**3, 3, n, 3 * n, plan.offsets)
+    qd = torch.empty(Q**3 * plan.num_elem, dtype=torch.float64, device=dev)
+    fem.mass_build(rx, fem.Basis(3, 3, P, Q), torch.from_numpy(coords).to(dev), qd)
+    op = fem.MassOperator(fem.Restriction(plan.num_elem, P**3, 1, n, n, plan.offsets), fem.Basis(3, 1, P, Q), qd)
+    del rx, coords
+    g = torch.Generator(device=dev).manual_seed(SEED)
+    u = torch.rand(n, dtype=torch.float64, device=dev, generator=g) * 2 - 1
+    v = torch.empty_like(u)
+    send = torch.empty(max(1, plan.shared_total), dtype=torch.float64, device=dev)
+    recv = torch.empty_like(send)
+    segs, s0 = [], 0
+    for q, idx in plan.peers:
+        segs.append((q, s0, len(idx)))
+        s0 += len(idx)
+
+    def exchange():
+        if not segs:
+            return
+        plan.pack(v, send[:plan.shared_total])
+        ops = []
+        for q, a, c in segs:
+            ops.append(dist.P2POp(dist.isend, send[a:a + c], q))
+            ops.append(dist.P2POp(dist.irecv, recv[a:a + c], q))
+        for req in dist.batch_isend_irecv(ops):
+            req.wait()
+        plan.unpack_add(recv[:plan.shared_total], v)
+
+    stream = torch.cuda.current_stream()
+    for _ in range(max(3, args.warmup)):
+        op.apply(u, v)
+        exchange()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    K = args.steps
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(3 * K)]
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for i in range(K):
+        e[3 * i].record(stream)
+        op.apply(u, v)
+        e[3 * i + 1].record(stream)
+        exchange()
+        e[3 * i + 2].record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    wall = (time.perf_counter() - t0) / K * 1e3
+    apply_ms = sum(e[3 * i].elapsed_time(e[3 * i + 1]) for i in range(K)) / K
+    exch_ms = sum(e[3 * i + 1].elapsed_time(e[3 * i + 2]) for i in range(K)) / K
+    step_ms = apply_ms + exch_ms
+    t = torch.tensor([step_ms, apply_ms, exch_ms, wall], dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    step_ms, apply_max, exch_max, wall = t.tolist()
+    xbytes = torch.tensor([8.0 * plan.shared_total], dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(xbytes)
+    line = {"split": "mass_apply", "metric": "GDoF/s operator_apply, one mesh over the ranks",
+            "value": N / (step_ms * 1e-3) / 1e9, "unit": "GDoF/s", "n_gpus": world, "steps": K,
+            "ms_per_step": step_ms, "scaling": "strong", "higher_is_better": True,
+            "per_rank_max": {"apply_ms": apply_max, "exchange_ms": exch_max, "wall_ms": wall},
+            "exchange_bytes_per_step_all_ranks": xbytes.item(),
+            "config": {"workload": WORKLOAD, "mesh": "x".join(map(str, SHAPE)), "P": P, "Q": Q, "dofs": N,
+                       "partition": "contiguous element ranges (fem_b200_shard_*)",
+                       "exchange": "device pack, NCCL batch_isend_irecv of the shared values, rank-ordered "
+                                   "unpack-add (same bits on every rank)"}}
+    return line
+
+
 def run_e2e_sweep(args):
     import torch
     import fe_demo_cpp_b200 as fem
@@ -982,6 +1090,8 @@ def main():
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-orders", action="store_true", help="skip the P = 2..4 roofline fractions")
+    ap.add_argument("--split", action="store_true",
+                    help="one mesh over the ranks: element ranges, interface exchange over NCCL (extra line)")
     ap.add_argument("--orders-steps", type=int, default=20)
     ap.add_argument("--cpu-sample-s", type=float, default=12.0, help="approximate CPU seconds of the baseline")
     ap.add_argument("--shape", default=None, help="elements per direction nx,ny,nz (default 100,100,100)")
@@ -1051,7 +1161,7 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local_rank))
-    line = run_b200(args, rank, world, local_rank)
+    line = run_split(args, rank, world, local_rank) if args.split else run_b200(args, rank, world, local_rank)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -19,6 +19,7 @@ from .api import (  # noqa: F401
     Restriction,
     ScatterMode,
     Server,
+    ShardPlan,
     check_offset_restriction,
     check_strided_restriction,
     gauss_legendre_quadrature,

@@ -76,6 +76,13 @@ SIGNATURES = {
     "fem_b200_batch_autotune": ([_p, _i, _p], _i),
     "fem_b200_batch_set_mode": ([_p, _i], _i),
     "fem_b200_batch_check": ([_p, _p], _i),
+    "fem_b200_shard_create": ([_i, _i, _p, _i, _i, _p], _i),
+    "fem_b200_shard_sizes": ([_p, _p, _p, _p, _p, _p], _i),
+    "fem_b200_shard_local": ([_p, _p, _p, _p], _i),
+    "fem_b200_shard_peer": ([_p, _i, _p, _p, _p], _i),
+    "fem_b200_shard_pack": ([_p, _p, _i64, _i, _p, _i64, _p], _i),
+    "fem_b200_shard_unpack_add": ([_p, _p, _i64, _i, _p, _i64, _p], _i),
+    "fem_b200_shard_destroy": ([_p], _i),
     "fem_b200_batch_info": ([_p, _p, _p, _p, _p, _p, _p], _i),
     "fem_b200_batch_destroy": ([_p], _i),
     "fem_b200_server_create": ([_i, _i64, _p], _i),

@@ -511,3 +511,46 @@ class Server(_Handle):
              C.addressof(pend), C.addressof(use), C.addressof(peak))
         return {"submitted": sub.value, "completed": comp.value, "running": run.value, "pending": pend.value,
                 "bytes_in_use": use.value, "bytes_peak": peak.value}
+
+
+class ShardPlan(_Handle):
+    """This rank's part of a mesh split into contiguous element ranges, through
+    the C ABI (fem_b200_shard_*): sizes, the compact local numbering, the
+    nodes shared with each peer, and the device pack / rank-ordered
+    unpack-add of the interface exchange (the caller moves the segments)."""
+    _destroy = "fem_b200_shard_destroy"
+
+    def __init__(self, offsets, elem_size: int, world: int, rank: int):
+        super().__init__()
+        offsets = np.ascontiguousarray(offsets, dtype=np.int32)
+        call("fem_b200_shard_create", offsets.size // elem_size, elem_size, _ptr(offsets), int(world), int(rank),
+             C.addressof(self.h))
+        e0, e1, nn, npeer = C.c_int(0), C.c_int(0), C.c_int(0), C.c_int(0)
+        tot = C.c_int64(0)
+        call("fem_b200_shard_sizes", self.h, C.addressof(e0), C.addressof(e1), C.addressof(nn), C.addressof(npeer),
+             C.addressof(tot))
+        self.e0, self.e1, self.num_nodes, self.shared_total = e0.value, e1.value, nn.value, tot.value
+        self.num_elem = self.e1 - self.e0
+        self.offsets = np.zeros(self.num_elem * elem_size, np.int32)
+        self.l2g = np.zeros(self.num_nodes, np.int64)
+        owned = np.zeros(self.num_nodes, np.uint8)
+        call("fem_b200_shard_local", self.h, _ptr(self.offsets), _ptr(self.l2g), _ptr(owned))
+        self.owned = owned.astype(bool)
+        self.peers = []  # (peer rank, local indices)
+        for i in range(npeer.value):
+            q, cnt = C.c_int(0), C.c_int64(0)
+            call("fem_b200_shard_peer", self.h, i, C.addressof(q), C.addressof(cnt), None)
+            idx = np.zeros(cnt.value, np.int64)
+            call("fem_b200_shard_peer", self.h, i, None, None, _ptr(idx))
+            self.peers.append((q.value, idx))
+
+    def pack(self, v, send, num_comp=1, stream=None):
+        _check_dev(v)
+        _check_dev(send)
+        call("fem_b200_shard_pack", self.h, _ptr(v), _n(v), int(num_comp), _ptr(send), _n(send), _stream(stream))
+
+    def unpack_add(self, recv, v, num_comp=1, stream=None):
+        _check_dev(recv)
+        _check_dev(v)
+        call("fem_b200_shard_unpack_add", self.h, _ptr(recv), _n(recv), int(num_comp), _ptr(v), _n(v),
+             _stream(stream))

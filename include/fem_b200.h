@@ -482,6 +482,41 @@ int fem_b200_mass_apply_bf16_tc(fem_b200_mass op, const void *u_bf16, int64_t n_
  * descriptors and layouts are right). */
 int fem_b200_tc_selftest(double *max_rel_err);
 
+/* ---- one mesh over several ranks (no reference counterpart; the reference
+ * is single-process, src/operator.cpp:148-182) ---------------------------------
+ * The elements are split into `world` contiguous ranges; rank `rank` holds
+ * elements [e0, e1) with its nodes renumbered compactly in ascending global
+ * id (l2g), applies the mass operator to them (an operator over
+ * local_offsets), then sums the values of the nodes it shares with other
+ * ranks.  The sum needs one exchange per apply: fem_b200_shard_pack puts the
+ * shared values, for every peer, into one send buffer (peer i's segment is
+ * contiguous: count_i x num_comp values from offset num_comp x (the counts
+ * of peers before i)); the caller moves each segment to its peer and fills
+ * the receive buffer in the same layout (NCCL send/recv, MPI, a copy);
+ * fem_b200_shard_unpack_add then sets every shared value to the sum of all
+ * ranks' values in rank order, from 0, so a shared node ends with the same
+ * bits on every rank.  A node is owned by the lowest rank that touches it
+ * (for dot products over the whole mesh).  Vectors are blocked
+ * [num_comp][num_nodes]; pack / unpack take device pointers.  The set-up
+ * reads the whole mesh's offsets on the host and needs no GPU. */
+typedef struct fem_b200_shard_s *fem_b200_shard;
+int fem_b200_shard_create(int num_elem, int elem_size, const int *offsets, int world, int rank,
+                          fem_b200_shard *out);
+/* Any output may be NULL.  shared_total: the sum of the peers' counts. */
+int fem_b200_shard_sizes(fem_b200_shard s, int *e0, int *e1, int *num_nodes, int *num_peers,
+                         int64_t *shared_total);
+/* local_offsets [(e1 - e0) * elem_size], l2g [num_nodes], owned [num_nodes]
+ * (1 where this rank owns the node); any may be NULL. */
+int fem_b200_shard_local(fem_b200_shard s, int *local_offsets, int64_t *l2g, unsigned char *owned);
+/* Peer i (ascending rank): its rank, the number of shared nodes, their local
+ * indices (ascending; may be NULL). */
+int fem_b200_shard_peer(fem_b200_shard s, int i, int *peer, int64_t *count, int64_t *local_idx);
+int fem_b200_shard_pack(fem_b200_shard s, const double *v, int64_t n_v, int num_comp, double *send, int64_t n_send,
+                        void *stream);
+int fem_b200_shard_unpack_add(fem_b200_shard s, const double *recv, int64_t n_recv, int num_comp, double *v,
+                              int64_t n_v, void *stream);
+int fem_b200_shard_destroy(fem_b200_shard s);
+
 /* Synchronise `stream` and report a device-side failure of the plan's kernels
  * (a bounded wait that ran out) as FEM_B200_ERROR_CUDA.  fem_b200_mass_apply_host
  * does this check itself. */
