@@ -192,10 +192,12 @@ struct Mass3D {
   static constexpr int SB = cmax(P * PS2, Q * PS4);
   static constexpr int SMEM = (SA + SB) * 8;
   static constexpr int ES = P * P * P, NQ = Q * Q * Q;
-  // resident CTAs per SM the register-capped variant asks for: 5, or what
-  // shared memory (227 KB) and threads (2048) allow
-  static constexpr int MINB_OCC = cmax(1, (5 < 232448 / SMEM ? 5 : 232448 / SMEM) < 2048 / NT
-                                              ? (5 < 232448 / SMEM ? 5 : 232448 / SMEM)
+  // resident CTAs per SM the register-capped variant asks for: 8 at
+  // P <= 4 (narrow tiles: 72-200 threads), 5 above, or what shared memory
+  // (227 KB) and threads (2048) allow
+  static constexpr int OCC_CAP = P <= 4 ? 8 : 5;
+  static constexpr int MINB_OCC = cmax(1, (OCC_CAP < 232448 / SMEM ? OCC_CAP : 232448 / SMEM) < 2048 / NT
+                                              ? (OCC_CAP < 232448 / SMEM ? OCC_CAP : 232448 / SMEM)
                                               : 2048 / NT);
 };
 
