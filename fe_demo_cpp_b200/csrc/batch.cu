@@ -208,12 +208,12 @@ __device__ __forceinline__ void persist_tiles(const PersistMats<T>& mats, const 
   const int64_t tile = tile0 + (in_group ? g : 0);
   if constexpr (D == 3) {
     using L = Mass3D<P, Q>;
-    mass3d_tile<P, Q, T, ApplyPlain, 1, T, Mat1D<P, Q, T>, persist_even_odd<P, T>()>(
+    mass3d_tile<P, Q, T, ApplyPlain, 1, T, Mat1D<P, Q, T>, persist_even_odd<P, T>(), true>(
         persist_mat<P>(mats), base, base + L::SA, mm.offs, mm.qd, mm.u, mm.v, nullptr, mm.num_elem, mm.comp_run,
         mm.comp_stride, ApplyPlain{}, tile, dsum, t);
   } else {
     using L = Mass2D<P, Q>;
-    mass2d_tile<P, Q, T, ApplyPlain, T, Mat1D<P, Q, T>, false>(persist_mat<P>(mats), base, base + L::S1, mm.offs,
+    mass2d_tile<P, Q, T, ApplyPlain, T, Mat1D<P, Q, T>, false, true>(persist_mat<P>(mats), base, base + L::S1, mm.offs,
                                                                mm.qd, mm.u, mm.v, nullptr, mm.num_elem, mm.comp_run,
                                                                mm.comp_stride, ApplyPlain{}, tile, dsum, t);
   }

@@ -95,17 +95,6 @@ void launch_apply3_kernel(const MassPlan& p, const double* u, double* v, double*
   FEM_LAUNCH_CHECK();
 }
 
-// The register-capped variant: the simple kernel's contractions (even-odd
-// where it takes them) at MINB_OCC resident CTAs a SM.
-template <int P, int Q>
-void launch_apply3_occ(const MassPlan& p, const double* u, double* v, double* ev, cudaStream_t s) {
-  if constexpr (plain_even_odd<P>()) {
-    if (p.centro_symmetric)
-      return launch_apply3_kernel<P, Q, Mass3D<P, Q>::MINB_OCC, false, true>(p, u, v, ev, s);
-  }
-  launch_apply3_kernel<P, Q, Mass3D<P, Q>::MINB_OCC, false, false>(p, u, v, ev, s);
-}
-
 // Persistent grid: SMs x resident CTAs (from the occupancy calculator), at
 // most one CTA per tile.
 template <class K>
@@ -262,7 +251,7 @@ struct Table {
     if constexpr (Pipe3D<P, Q>::SMEM <= kMaxSmemPerCta) pp[P][DQ] = launch_apply3_pipe<P, Q>;
     if constexpr (Mass3DX2<P, Q>::SMEM <= kMaxSmemPerCta && Mass3DX2<P, Q>::NT <= 1024) xx[P][DQ] = launch_apply3_x2<P, Q>;
     if constexpr (Prefetch3D<P, Q>::SMEM <= kMaxSmemPerCta) pf[P][DQ] = launch_apply3_pf<P, Q>;
-    if constexpr (Mass3D<P, Q>::MINB_OCC > 1) oc[P][DQ] = launch_apply3_occ<P, Q>;
+    if constexpr (Mass3D<P, Q>::MINB_OCC > 1) oc[P][DQ] = launch_apply3_kernel<P, Q, Mass3D<P, Q>::MINB_OCC, false, false>;
     if constexpr (Narrow3D<P, Q>::SMEM <= kMaxSmemPerCta) nw[P][DQ] = launch_apply3_narrow<P, Q>;
     if constexpr (P <= 3) el[P][DQ] = launch_apply3_element<P, Q>;  // registers: 86 (P=2), 250 (P=3)
     bd[0][P][DQ] = launch_build1<P, Q>;

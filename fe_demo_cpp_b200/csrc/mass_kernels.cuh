@@ -192,12 +192,11 @@ struct Mass3D {
   static constexpr int SB = cmax(P * PS2, Q * PS4);
   static constexpr int SMEM = (SA + SB) * 8;
   static constexpr int ES = P * P * P, NQ = Q * Q * Q;
-  // resident CTAs per SM the register-capped variant asks for: 8 at
-  // P <= 4 (narrow tiles: 72-200 threads), 5 above, or what shared memory
-  // (227 KB) and threads (2048) allow
-  static constexpr int OCC_CAP = P <= 4 ? 8 : 5;
-  static constexpr int MINB_OCC = cmax(1, (OCC_CAP < 232448 / SMEM ? OCC_CAP : 232448 / SMEM) < 2048 / NT
-                                              ? (OCC_CAP < 232448 / SMEM ? OCC_CAP : 232448 / SMEM)
+  // resident CTAs per SM the register-capped variant asks for: 5, or what
+  // shared memory (227 KB) and threads (2048) allow (8 at P = 4, with the
+  // even-odd contractions, measured 1.096 ms against 0.973 ms at 5)
+  static constexpr int MINB_OCC = cmax(1, (5 < 232448 / SMEM ? 5 : 232448 / SMEM) < 2048 / NT
+                                              ? (5 < 232448 / SMEM ? 5 : 232448 / SMEM)
                                               : 2048 / NT);
 };
 
@@ -220,7 +219,8 @@ __device__ __forceinline__ void prefetch_tile_l2(const int* offs, const S* qd, i
 
 // One 8-element tile of the 3D fused apply (the body of mass3d_apply_kernel and
 // of the batched kernels): sa / sb are the CTA's shared buffers A and B.
-template <int P, int Q, class T, class Ext, int NCB, class S = T, class M = Mat1D<P, Q, T>, bool EO = false>
+template <int P, int Q, class T, class Ext, int NCB, class S = T, class M = Mat1D<P, Q, T>, bool EO = false,
+          bool GROUPED = false>
 __device__ __forceinline__ void mass3d_tile(const M& m, T* __restrict__ sa, T* __restrict__ sb,
                                             const int* __restrict__ offs, const S* __restrict__ qd,
                                             const S* __restrict__ u, T* __restrict__ v, T* __restrict__ ev,
@@ -228,11 +228,11 @@ __device__ __forceinline__ void mass3d_tile(const M& m, T* __restrict__ sa, T* _
                                             const Ext& ext, const int64_t tile, double& dsum, int t_in = -1) {
   using L = Mass3D<P, Q>;
   constexpr int E = L::E;
-  // t_in: the thread's index in a group of L::NT running this tile (a block
-  // may run several tiles, or have threads to spare: t_in >= L::NT only
-  // takes part in the barriers)
-  const int t = t_in < 0 ? int(threadIdx.x) : t_in, e = t % E, col = t / E;
-  const bool live = t < L::NT;
+  // GROUPED: t_in is the thread's index in a group of L::NT running this
+  // tile (a block may run several tiles, or have threads to spare: t_in >=
+  // L::NT only takes part in the barriers); otherwise the block is the tile
+  const int t = GROUPED ? t_in : int(threadIdx.x), e = t % E, col = t / E;
+  const bool live = GROUPED ? t < L::NT : true;
   const bool nodal = col < P * P;  // (px, py) = (col % P, col / P)
   const bool mixed = col < P * Q;  // (px, qz) = (col % P, col / P)
   const int64_t eg = tile * E + e;
@@ -616,7 +616,8 @@ struct Mass2D {
 };
 
 // One 32-element tile of the 2D fused apply: s1 / s3 the CTA's shared buffers.
-template <int P, int Q, class T, class Ext, class S = T, class M = Mat1D<P, Q, T>, bool EO = false>
+template <int P, int Q, class T, class Ext, class S = T, class M = Mat1D<P, Q, T>, bool EO = false,
+          bool GROUPED = false>
 __device__ __forceinline__ void mass2d_tile(const M& m, T* __restrict__ s1, T* __restrict__ s3,
                                             const int* __restrict__ offs, const S* __restrict__ qd,
                                             const S* __restrict__ u, T* __restrict__ v, T* __restrict__ ev,
@@ -624,9 +625,9 @@ __device__ __forceinline__ void mass2d_tile(const M& m, T* __restrict__ s1, T* _
                                             const Ext& ext, const int64_t tile, double& dsum, int t_in = -1) {
   using L = Mass2D<P, Q>;
   constexpr int E = L::E;
-  // t_in: as mass3d_tile's (t_in >= L::NT: barriers only)
-  const int t = t_in < 0 ? int(threadIdx.x) : t_in, e = t % E, col = t / E;
-  const bool live = t < L::NT;
+  // GROUPED, t_in: as mass3d_tile's (t_in >= L::NT: barriers only)
+  const int t = GROUPED ? t_in : int(threadIdx.x), e = t % E, col = t / E;
+  const bool live = GROUPED ? t < L::NT : true;
   const bool nodal = col < P;
   const int64_t eg = tile * E + e;
   const bool valid = eg < num_elem;
