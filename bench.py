@@ -528,12 +528,15 @@ def run_sweep(args):
 # mass), f ~ U[-1,1], rtol 1e-10; FP64 PCG against FP32 PCG inside FP64
 # iterative refinement (extra JSON lines)
 # ---------------------------------------------------------------------------
-def cg_iteration_bytes(ne, n, P, Q, s, nc):
-    """Compulsory HBM bytes of one Chronopoulos-Gear PCG iteration with s-byte
-    vectors and qdata: the vector update reads dinv, r, p, s, w, x and writes
-    p, s, w, x, r (11 n s); the apply reads offsets and qdata per element,
-    gathers r (n s) and one dinv per node (n s / nc) and adds into w (2 n s)."""
-    return 11 * n * s + 3 * n * s + n * s // nc + ne * (4 * P**3 + s * Q**3)
+def cg_iteration_bytes(ne, n, P, Q, prec, nc):
+    """Compulsory HBM bytes of one Chronopoulos-Gear PCG iteration: k-byte
+    r, p, s and qdata, f-byte x, w and dinv (fp64: 8/8, fp32_ir: 4/4,
+    bf16_ir: 2/4).  The vector update reads dinv, r, p, s, w, x and writes
+    p, s, w, x, r (6 k + 5 f per entry); the apply reads offsets and qdata
+    per element, gathers r (k) and one dinv per node (f / nc) and adds into
+    w (2 f)."""
+    k, f = {"fp64": (8, 8), "fp32_ir": (4, 4), "bf16_ir": (2, 4)}[prec]
+    return n * (6 * k + 5 * f) + n * (k + 2 * f) + n * f // nc + ne * (4 * P**3 + k * Q**3)
 
 
 def run_solve(args):
@@ -564,7 +567,7 @@ def run_solve(args):
     f = torch.rand(n, dtype=torch.float64, device=dev, generator=g) * 2 - 1
     results, sols = {}, {}
     sampler = ClockSampler(0).start()
-    for prec in ("fp64", "fp32_ir"):
+    for prec in ("fp64", "fp32_ir", "bf16_ir"):
         u = torch.empty_like(f)
         for _ in range(max(1, args.warmup // 3)):
             info = op.solve(f, u, rtol=args.solve_rtol, max_iter=2000, precision=prec)
@@ -593,7 +596,7 @@ def run_solve(args):
         sps = 1e3 / (sum(wall) / len(wall))
         base = sps if prec == "fp64" else base
         err = float((sols[prec] - ref).norm() / ref.norm())
-        it_bytes = cg_iteration_bytes(ne, n, Pp, Qq, 8 if prec == "fp64" else 4, nc)
+        it_bytes = cg_iteration_bytes(ne, n, Pp, Qq, prec, nc)
         print(json.dumps({
             "solve": "mass", "precision": prec, "metric": "solves/s", "value": sps, "unit": "solves/s",
             "p50_ms": p50, "p99_ms": p99, "device_ms_mean": mean_dev, "steps": len(wall),

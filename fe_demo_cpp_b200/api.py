@@ -39,6 +39,10 @@ class ScatterMode(IntEnum):
     Deterministic = 1
 
 
+# fem_b200_mass_solve's precision argument (FEM_B200_SOLVE_*)
+SOLVE_PRECISIONS = {"fp64": 0, "fp32_ir": 1, "bf16_ir": 2}
+
+
 class KernelVariant(IntEnum):
     auto = 0
     simple = 1
@@ -350,11 +354,12 @@ class MassOperator(_Handle):
         call("fem_b200_mass_diagonal", self.h, _ptr(diag), _n(diag), _stream(stream))
 
     def solve(self, f, u, rtol=1e-10, max_iter=1000, precision="fp64", stream=None) -> dict:
-        """Solve M u = f (device arrays) by Jacobi PCG; precision 'fp64' or
-        'fp32_ir' (FP32 inner PCG in FP64 iterative refinement)."""
+        """Solve M u = f (device arrays) by Jacobi PCG; precision 'fp64',
+        'fp32_ir' (FP32 inner PCG in FP64 iterative refinement) or 'bf16_ir'
+        (BF16-storage inner PCG, FP32 arithmetic, in FP64 refinement)."""
         _check_dev(f)
         _check_dev(u)
-        prec = {"fp64": 0, "fp32_ir": 1}[precision]
+        prec = SOLVE_PRECISIONS[precision]
         its, outer, rel = C.c_int(0), C.c_int(0), C.c_double(0.0)
         call("fem_b200_mass_solve", self.h, _ptr(f), _n(f), _ptr(u), _n(u), float(rtol), int(max_iter), prec,
              C.addressof(its), C.addressof(outer), C.addressof(rel), _stream(stream))
@@ -458,7 +463,7 @@ class Server(_Handle):
     def _common(req, dim, P, Q, num_comp, rtol, max_iter, precision, deterministic, u_out, f_out):
         req.dim, req.P, req.Q, req.num_comp = int(dim), int(P), int(Q if Q is not None else P + 1), int(num_comp)
         req.rtol, req.max_iter = float(rtol), int(max_iter)
-        req.precision = {"fp64": 0, "fp32_ir": 1}[precision]
+        req.precision = SOLVE_PRECISIONS[precision]
         req.scatter_mode = 1 if deterministic else 0
         for name, a in (("u_out", u_out), ("f_out", f_out)):
             if a is not None:

@@ -32,14 +32,18 @@
 
 namespace fem_b200 {
 
-// A value of storage type S read as compute type T (S = T, or BF16 storage
-// of u and qdata under FP32 arithmetic).
+// A value of storage type S as compute type T (S = T, or BF16 storage of u
+// and qdata under FP32 arithmetic).
+template <class T, class S>
+__device__ __forceinline__ T as_t(S x) {
+  if constexpr (std::is_same<S, __nv_bfloat16>::value)
+    return T(__bfloat162float(x));
+  else
+    return T(x);
+}
 template <class T, class S>
 __device__ __forceinline__ T load_as(const S* p) {
-  if constexpr (std::is_same<S, __nv_bfloat16>::value)
-    return T(__bfloat162float(*p));
-  else
-    return T(__ldg(p));
+  return as_t<T>(__ldg(p));
 }
 
 template <int P, int Q, class T = double>

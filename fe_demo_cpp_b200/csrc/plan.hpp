@@ -253,7 +253,8 @@ struct MassPlan {
   CgScalars* cg_host_ext = nullptr;       // or a page-locked copy owned by the caller (a server slot)
   DevBuf<float> qd_t32, dinv32, evec32;   // FP32 copies (inner solves, FP32 applies)
   DevBuf<__nv_bfloat16> qd_t16;           // BF16 qdata (BF16-storage applies)
-  DevBuf<float> f_r, f_p, f_s, f_w, f_x;  // FP32 Krylov vectors
+  DevBuf<float> f_r, f_p, f_s, f_w, f_x;  // FP32 Krylov vectors (f_w, f_x: also the BF16 solve's)
+  DevBuf<__nv_bfloat16> h_r, h_p, h_s;    // BF16 Krylov vectors
   DevBuf<int> tc_ticket;                  // tile counter of the tensor-core apply (zeroed before each launch)
 };
 

@@ -249,7 +249,8 @@ class SolveServer {
     require(r.num_comp >= 1 && r.num_comp <= 3, "server submit: num_comp must be 1..3");
     require(r.rtol > 0.0 && r.rtol < 1.0, "server submit: rtol must be in (0, 1)");
     require(r.max_iter >= 1, "server submit: max_iter must be positive");
-    require(r.precision == FEM_B200_SOLVE_FP64 || r.precision == FEM_B200_SOLVE_FP32_IR,
+    require(r.precision == FEM_B200_SOLVE_FP64 || r.precision == FEM_B200_SOLVE_FP32_IR ||
+                r.precision == FEM_B200_SOLVE_BF16_IR,
             "server submit: unknown precision");
     require(r.scatter_mode == FEM_B200_SCATTER_ATOMIC || r.scatter_mode == FEM_B200_SCATTER_DETERMINISTIC,
             "server submit: unknown scatter mode");

@@ -4,11 +4,13 @@
 //     stay on the device, so the host queues iterations without waiting;
 //     the Jacobi scaling is folded into the apply's gather and (u, M u) into
 //     its quadrature-point pass (apply_ext.cuh);
-//   * FP64 PCG, and FP32 PCG inside FP64 iterative refinement.
+//   * FP64 PCG, and FP32 PCG or BF16-storage PCG (FP32 arithmetic) inside
+//     FP64 iterative refinement.
 // Reductions accumulate in FP64 in every precision, in a fixed order; the
 // outer residual of the refinement is an FP64 apply.  The reference has no
 // solver: these solve M u = f with its mass operator and are tested against
 // the oracle's apply (f = M u* for a known u*).
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -249,6 +251,113 @@ __global__ void cg_update_kernel(int64_t n, const T* __restrict__ dinv, T* __res
   });
 }
 
+// ---- BF16-storage inner PCG (FEM_B200_SOLVE_BF16_IR) -----------------------
+// r, p, s stored in BF16 (2 bytes an entry); x (the correction, whose
+// rounding would stay in the refined solution), w (the apply's atomic target)
+// and dinv in FP32; FP32 arithmetic, FP64 reductions: the same recurrences as
+// cg_init_kernel / cg_update_kernel.
+using bf16 = __nv_bfloat16;
+
+__global__ void cg_init_bf16_kernel(int64_t n, const double* __restrict__ b, double scale,
+                                    const float* __restrict__ dinv, float* __restrict__ x, bf16* __restrict__ r,
+                                    bf16* __restrict__ p, bf16* __restrict__ sv, float* __restrict__ w,
+                                    CgScalars* st, double* part, double rtol, int max_iters) {
+  double v[2] = {0.0, 0.0};
+  const bf16 zero = __float2bfloat16_rn(0.0f);
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    const bf16 rb = __float2bfloat16_rn(float(b[i] * scale));
+    const float ri = __bfloat162float(rb);
+    x[i] = 0.0f, p[i] = zero, sv[i] = zero, w[i] = 0.0f;
+    r[i] = rb;
+    v[0] += double(ri) * double(dinv[i] * ri);
+    v[1] += double(ri) * double(ri);
+  }
+  grid_sum<2>(v, part, &st->ticket, [&](const double* tot) {
+    st->gamma = tot[0], st->gamma_old = tot[0];
+    st->rr = tot[1], st->rr0 = tot[1];
+    st->tol2 = rtol * rtol * tot[1];
+    st->alpha = 0.0, st->beta = 0.0, st->delta = 0.0;
+    st->iters = 0, st->max_iters = max_iters;
+    st->done = tot[1] > 0.0 ? 0 : 1;
+  });
+}
+
+// Eight entries a thread: one 16-byte access to each BF16 vector, two to each
+// FP32 one (vec: every vector 16-byte aligned, checked by the host; the
+// scalar loop takes the entries past the last multiple of 8).
+__global__ void cg_update_bf16_kernel(int64_t n, const float* __restrict__ dinv, float* __restrict__ x,
+                                      bf16* __restrict__ r, bf16* __restrict__ p, bf16* __restrict__ sv,
+                                      float* __restrict__ w, CgScalars* st, double* part, bool vec) {
+  if (st->done) return;
+  const float a = float(st->alpha), bt = float(st->beta);
+  double v[2] = {0.0, 0.0};
+  auto step = [&](float di, float& ri, float& pi, float& si, float& wi, float& xi) {
+    pi = di * ri + bt * pi;
+    si = wi + bt * si;
+    wi = 0.0f;
+    xi += a * pi;
+    ri = ri - a * si;
+  };
+  const int64_t tid = blockIdx.x * int64_t(blockDim.x) + threadIdx.x, stride = int64_t(gridDim.x) * blockDim.x;
+  int64_t head = 0;
+  if (vec) {
+    const int64_t nv = n / 8;
+    for (int64_t j = tid; j < nv; j += stride) {
+      uint4 R = reinterpret_cast<const uint4*>(r)[j], Pv = reinterpret_cast<const uint4*>(p)[j];
+      uint4 S = reinterpret_cast<const uint4*>(sv)[j];
+      float4 X0 = reinterpret_cast<const float4*>(x)[2 * j], X1 = reinterpret_cast<const float4*>(x)[2 * j + 1];
+      float4 D0 = reinterpret_cast<const float4*>(dinv)[2 * j], D1 = reinterpret_cast<const float4*>(dinv)[2 * j + 1];
+      float4 W0 = reinterpret_cast<const float4*>(w)[2 * j], W1 = reinterpret_cast<const float4*>(w)[2 * j + 1];
+      bf16* rb = reinterpret_cast<bf16*>(&R);
+      bf16* pb = reinterpret_cast<bf16*>(&Pv);
+      bf16* sb = reinterpret_cast<bf16*>(&S);
+      float xx[8] = {X0.x, X0.y, X0.z, X0.w, X1.x, X1.y, X1.z, X1.w};
+      const float dd[8] = {D0.x, D0.y, D0.z, D0.w, D1.x, D1.y, D1.z, D1.w};
+      float ww[8] = {W0.x, W0.y, W0.z, W0.w, W1.x, W1.y, W1.z, W1.w};
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        float ri = __bfloat162float(rb[k]), pi = __bfloat162float(pb[k]), si = __bfloat162float(sb[k]);
+        step(dd[k], ri, pi, si, ww[k], xx[k]);
+        rb[k] = __float2bfloat16_rn(ri), pb[k] = __float2bfloat16_rn(pi), sb[k] = __float2bfloat16_rn(si);
+        const float rr = __bfloat162float(rb[k]);
+        v[0] += double(rr) * double(dd[k] * rr);
+        v[1] += double(rr) * double(rr);
+      }
+      reinterpret_cast<uint4*>(r)[j] = R, reinterpret_cast<uint4*>(p)[j] = Pv;
+      reinterpret_cast<uint4*>(sv)[j] = S;
+      reinterpret_cast<float4*>(x)[2 * j] = make_float4(xx[0], xx[1], xx[2], xx[3]);
+      reinterpret_cast<float4*>(x)[2 * j + 1] = make_float4(xx[4], xx[5], xx[6], xx[7]);
+      reinterpret_cast<float4*>(w)[2 * j] = make_float4(0.f, 0.f, 0.f, 0.f);
+      reinterpret_cast<float4*>(w)[2 * j + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    head = nv * 8;
+  }
+  for (int64_t i = head + tid; i < n; i += stride) {
+    float ri = __bfloat162float(r[i]), pi = __bfloat162float(p[i]), si = __bfloat162float(sv[i]);
+    float wi = w[i], xi = x[i];
+    step(dinv[i], ri, pi, si, wi, xi);
+    r[i] = __float2bfloat16_rn(ri), p[i] = __float2bfloat16_rn(pi), sv[i] = __float2bfloat16_rn(si);
+    w[i] = wi, x[i] = xi;
+    const float rr = __bfloat162float(r[i]);
+    v[0] += double(rr) * double(dinv[i] * rr);
+    v[1] += double(rr) * double(rr);
+  }
+  grid_sum<2>(v, part, &st->ticket, [&](const double* tot) {
+    st->gamma_old = st->gamma, st->gamma = tot[0];
+    st->rr = tot[1];
+    st->iters += 1;
+    if (tot[1] <= st->tol2)
+      st->done = 1;
+    else if (st->iters >= st->max_iters)
+      st->done = 2;
+  });
+}
+
+__global__ void to_bf16_kernel(int64_t n, const double* __restrict__ in, bf16* __restrict__ out) {
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    out[i] = __float2bfloat16_rn(float(in[i]));
+}
+
 // diag[off + k*comp_stride] = diag[off] for the components k >= 1 of every
 // element node: the mass diagonal is the same for every component.
 __global__ void broadcast_comp_kernel(int64_t n, const int* __restrict__ offsets, int num_comp, int64_t comp_stride,
@@ -293,8 +402,8 @@ __global__ void to_float_kernel(int64_t n, const double* __restrict__ in, float*
 // dispatch of the diagonal and CG apply kernels over the compiled (P, Q) set
 // ---------------------------------------------------------------------------
 using DiagLauncher = void (*)(const MassPlan&, double*, double*, cudaStream_t);
-template <class T>
-using CgApplyLauncher = void (*)(const MassPlan&, const T*, T*, T*, const T*, const ApplyCg<T>&, cudaStream_t);
+template <class T, class S = T>
+using CgApplyLauncher = void (*)(const MassPlan&, const S*, T*, T*, const S*, const ApplyCg<T>&, cudaStream_t);
 
 template <int P, int Q>
 Mat1D<P, Q> squared_mat(const BasisData& b) {
@@ -353,8 +462,8 @@ unsigned resident_grid(K kernel, int threads, int smem, int64_t n_tiles) {
 
 // w (+)= M (dinv . r) with delta = (dinv . r)^T M (dinv . r) reduced into the
 // solver scalars.  ev != nullptr: element contributions to the E-vector.
-template <int P, int Q, class T, int NCB, bool EO = (P == 4 || P >= 6) && sizeof(T) == 8 && NCB == 1>
-void launch_cg_apply3(const MassPlan& p, const T* r, T* w, T* ev, const T* qd, const ApplyCg<T>& ext,
+template <int P, int Q, class T, int NCB, class S = T, bool EO = (P == 4 || P >= 6) && sizeof(T) == 8 && NCB == 1>
+void launch_cg_apply3(const MassPlan& p, const S* r, T* w, T* ev, const S* qd, const ApplyCg<T>& ext,
                       cudaStream_t s) {
   using L = Mass3D<P, Q>;
   constexpr int smem = NCB * (L::SA + L::SB) * int(sizeof(T));
@@ -365,10 +474,10 @@ void launch_cg_apply3(const MassPlan& p, const T* r, T* w, T* ev, const T* qd, c
   // prefetches its next tile into L2 (FP64 solve 57.2 -> 56.5 ms at 64^3,
   // P = 5, 3 components; FP32 unchanged).
   if constexpr (EO) {
-    if (!p.centro_symmetric) return launch_cg_apply3<P, Q, T, NCB, false>(p, r, w, ev, qd, ext, s);
+    if (!p.centro_symmetric) return launch_cg_apply3<P, Q, T, NCB, S, false>(p, r, w, ev, qd, ext, s);
   }
   constexpr bool sb = P >= 7 && sizeof(T) == 8 && !EO;
-  const auto kern = mass3d_apply_kernel<P, Q, cg_min_blocks(L::NT, P, sb || (EO && P == 7)), T, ApplyCg<T>, NCB, T,
+  const auto kern = mass3d_apply_kernel<P, Q, cg_min_blocks(L::NT, P, sb || (EO && P == 7)), T, ApplyCg<T>, NCB, S,
                                         sb, EO>;
   set_smem(kern, smem, smem_set);
   kern<<<resident_grid(kern, L::NT, smem, p.n_tiles), L::NT, smem, s>>>(
@@ -376,33 +485,34 @@ void launch_cg_apply3(const MassPlan& p, const T* r, T* w, T* ev, const T* qd, c
   FEM_LAUNCH_CHECK();
 }
 
-template <int P, int Q, class T>
-void launch_cg_apply(const MassPlan& p, const T* r, T* w, T* ev, const T* qd, const ApplyCg<T>& ext,
+template <int P, int Q, class T, class S = T>
+void launch_cg_apply(const MassPlan& p, const S* r, T* w, T* ev, const S* qd, const ApplyCg<T>& ext,
                      cudaStream_t s) {
   if (p.dim == 3) {
     // FP32: components batched through the phases where shared memory allows;
     // FP64: one at a time.  64^3 hexes, P = 5, 3 components: FP32 solve 32.1
     // ms batched vs 34.7 ms one at a time; FP64 56.2 ms batched (3 resident
-    // CTAs, shared memory bound) vs 52.1 ms one at a time (4 CTAs).
+    // CTAs, shared memory bound) vs 52.1 ms one at a time (4 CTAs); BF16
+    // storage 41.6 ms batched vs 43.7 ms one at a time.
     constexpr int smem1 = (Mass3D<P, Q>::SA + Mass3D<P, Q>::SB) * int(sizeof(T));
     if constexpr (sizeof(T) == 4 && 3 * smem1 <= kMaxSmemPerCta) {
-      if (p.comp_run == 3) return launch_cg_apply3<P, Q, T, 3>(p, r, w, ev, qd, ext, s);
+      if (p.comp_run == 3) return launch_cg_apply3<P, Q, T, 3, S>(p, r, w, ev, qd, ext, s);
     }
     if constexpr (sizeof(T) == 4 && 2 * smem1 <= kMaxSmemPerCta) {
-      if (p.comp_run == 2) return launch_cg_apply3<P, Q, T, 2>(p, r, w, ev, qd, ext, s);
+      if (p.comp_run == 2) return launch_cg_apply3<P, Q, T, 2, S>(p, r, w, ev, qd, ext, s);
     }
-    return launch_cg_apply3<P, Q, T, 1>(p, r, w, ev, qd, ext, s);
+    return launch_cg_apply3<P, Q, T, 1, S>(p, r, w, ev, qd, ext, s);
   }
   if (p.dim == 2) {
     using L = Mass2D<P, Q>;
     constexpr int smem = (L::S1 + L::S3) * int(sizeof(T));
     static std::atomic<uint64_t> smem_set{0};
-    const auto kern = mass2d_apply_kernel<P, Q, T, ApplyCg<T>>;
+    const auto kern = mass2d_apply_kernel<P, Q, T, ApplyCg<T>, S>;
     set_smem(kern, smem, smem_set);
     kern<<<resident_grid(kern, L::NT, smem, p.n_tiles), L::NT, smem, s>>>(
         typed_mat<P, Q, T>(p.basis), p.offs_t.get(), qd, r, w, ev, p.num_elem, p.comp_run, p.comp_stride, ext, 0);
   } else {
-    const auto kern = mass1d_apply_kernel<P, Q, T, ApplyCg<T>>;
+    const auto kern = mass1d_apply_kernel<P, Q, T, ApplyCg<T>, S>;
     kern<<<resident_grid(kern, 128, 0, p.n_tiles), 128, 0, s>>>(
         typed_mat<P, Q, T>(p.basis), p.offs_t.get(), qd, r, w, ev, p.num_elem, p.comp_run, p.comp_stride, ext);
   }
@@ -415,6 +525,7 @@ struct SolveDispatch {
   DiagLauncher diag[kSolveMaxP + 1][kSolveQSpan] = {};
   CgApplyLauncher<double> cg64[kSolveMaxP + 1][kSolveQSpan] = {};
   CgApplyLauncher<float> cg32[kSolveMaxP + 1][kSolveQSpan] = {};
+  CgApplyLauncher<float, __nv_bfloat16> cg16[kSolveMaxP + 1][kSolveQSpan] = {};
 };
 
 template <int P, int DQ>
@@ -423,6 +534,7 @@ struct SolveTable {
     d.diag[P][DQ] = launch_diag<P, P + DQ>;
     d.cg64[P][DQ] = launch_cg_apply<P, P + DQ, double>;
     d.cg32[P][DQ] = launch_cg_apply<P, P + DQ, float>;
+    d.cg16[P][DQ] = launch_cg_apply<P, P + DQ, float, __nv_bfloat16>;
     if constexpr (DQ + 1 < kSolveQSpan)
       SolveTable<P, DQ + 1>::fill(d);
     else if constexpr (P + 1 <= kSolveMaxP)
@@ -466,10 +578,12 @@ void assemble_diagonal(MassPlan& p, double* diag, cudaStream_t s) {
   }
 }
 
-// The plan's solver state: diagonal and its inverse, FP32 copies of qdata
-// and dinv, Krylov vectors, reduction partials and the device scalars.
-void ensure_solver_state(MassPlan& p, bool fp32, cudaStream_t s) {
-  const size_t n = size_t(p.l_size);
+// The plan's solver state: diagonal and its inverse, FP32 dinv and the
+// reduced-precision qdata and Krylov vectors of the inner solves, reduction
+// partials and the device scalars.  Each part is keyed on its own buffer: an
+// FP32 or BF16 apply may have made the FP32 / BF16 qdata copy already.
+void ensure_solver_state(MassPlan& p, int precision, cudaStream_t s) {
+  const size_t n = size_t(p.l_size), nq = p.qd_t.size();
   if (p.diag.size() != n) {
     p.diag.alloc(n);
     assemble_diagonal(p, p.diag.get(), s);
@@ -482,16 +596,28 @@ void ensure_solver_state(MassPlan& p, bool fp32, cudaStream_t s) {
     FEM_CUDA_CHECK(cudaMemsetAsync(p.cg_st.get(), 0, sizeof(CgScalars), s));
     if (!p.cg_host_ext) p.cg_host.alloc(1);
   }
-  if (fp32 && p.qd_t32.size() != p.qd_t.size()) {
-    p.qd_t32.alloc(p.qd_t.size());
-    to_float_kernel<<<red_grid(int64_t(p.qd_t.size())), 256, 0, s>>>(int64_t(p.qd_t.size()), p.qd_t.get(),
-                                                                    p.qd_t32.get());
-    FEM_LAUNCH_CHECK();
+  if (precision == FEM_B200_SOLVE_FP64) return;
+  if (p.dinv32.size() != n) {
     p.dinv32.alloc(n);
     invert_kernel<float><<<red_grid(int64_t(n)), 256, 0, s>>>(int64_t(n), p.diag.get(), p.dinv32.get());
     FEM_LAUNCH_CHECK();
-    p.f_r.alloc(n), p.f_p.alloc(n), p.f_s.alloc(n), p.f_w.alloc(n), p.f_x.alloc(n);
-    if (deterministic(p)) p.evec32.alloc(p.evec.size());
+    p.f_w.alloc(n), p.f_x.alloc(n);
+  }
+  if (deterministic(p) && p.evec32.size() != p.evec.size()) p.evec32.alloc(p.evec.size());
+  if (precision == FEM_B200_SOLVE_FP32_IR) {
+    if (p.qd_t32.size() != nq) {
+      p.qd_t32.alloc(nq);
+      to_float_kernel<<<red_grid(int64_t(nq)), 256, 0, s>>>(int64_t(nq), p.qd_t.get(), p.qd_t32.get());
+      FEM_LAUNCH_CHECK();
+    }
+    if (p.f_r.size() != n) p.f_r.alloc(n), p.f_p.alloc(n), p.f_s.alloc(n);
+  } else {
+    if (p.qd_t16.size() != nq) {
+      p.qd_t16.alloc(nq);
+      to_bf16_kernel<<<red_grid(int64_t(nq)), 256, 0, s>>>(int64_t(nq), p.qd_t.get(), p.qd_t16.get());
+      FEM_LAUNCH_CHECK();
+    }
+    if (p.h_r.size() != n) p.h_r.alloc(n), p.h_p.alloc(n), p.h_s.alloc(n);
   }
 }
 
@@ -506,15 +632,20 @@ const CgScalars& read_scalars(MassPlan& p, cudaStream_t s) {
 
 inline bool aligned16(const void* ptr) { return (reinterpret_cast<uintptr_t>(ptr) & 15) == 0; }
 
-template <class T>
+// Krylov vectors r, p, s in storage S; x, w (the apply's target), the
+// E-vector and dinv in the arithmetic type T.
+template <class T, class S = T>
 struct Krylov {
-  T *x, *r, *p, *s, *w, *ev;
-  const T *dinv, *qd;
-  CgApplyLauncher<T> apply;
+  T* x;
+  S *r, *p, *s;
+  T *w, *ev;
+  const T* dinv;
+  const S* qd;
+  CgApplyLauncher<T, S> apply;
 };
 
-template <class T>
-void cg_apply(MassPlan& p, const Krylov<T>& k, cudaStream_t s) {
+template <class T, class S>
+void cg_apply(MassPlan& p, const Krylov<T, S>& k, cudaStream_t s) {
   const ApplyCg<T> ext{k.dinv, p.part.get(), p.cg_st.get()};
   if (!deterministic(p)) {
     k.apply(p, k.r, k.w, nullptr, k.qd, ext, s);
@@ -531,27 +662,34 @@ void cg_apply(MassPlan& p, const Krylov<T>& k, cudaStream_t s) {
 // max_it residual updates.  The host queues iterations in growing batches and
 // reads the scalars between batches; kernels queued after the stop return at
 // once.  Returns the final scalars.
-template <class T>
-CgScalars krylov_solve(MassPlan& p, const Krylov<T>& k, const double* b, double scale, double rtol, int max_it,
+template <class T, class S = T>
+CgScalars krylov_solve(MassPlan& p, const Krylov<T, S>& k, const double* b, double scale, double rtol, int max_it,
                        cudaStream_t s) {
+  constexpr bool mixed = !std::is_same<T, S>::value;
   const int64_t n = p.l_size;
   const int g = red_grid(n);
-  cg_init_kernel<T><<<g, 256, 0, s>>>(n, b, scale, k.dinv, k.x, k.r, k.p, k.s, k.w, p.cg_st.get(), p.part.get(),
-                                      rtol, max_it);
+  if constexpr (mixed)
+    cg_init_bf16_kernel<<<g, 256, 0, s>>>(n, b, scale, k.dinv, k.x, k.r, k.p, k.s, k.w, p.cg_st.get(), p.part.get(),
+                                          rtol, max_it);
+  else
+    cg_init_kernel<T><<<g, 256, 0, s>>>(n, b, scale, k.dinv, k.x, k.r, k.p, k.s, k.w, p.cg_st.get(), p.part.get(),
+                                        rtol, max_it);
   FEM_LAUNCH_CHECK();
-  cg_apply<T>(p, k, s);
+  cg_apply(p, k, s);
   const bool vec = aligned16(k.dinv) && aligned16(k.x) && aligned16(k.r) && aligned16(k.p) && aligned16(k.s) &&
                    aligned16(k.w);
   int batch = 4;
   for (int queued = 0;; queued += batch, batch = std::min(batch * 2, 32)) {
     for (int j = 0; j < batch; ++j) {
-      if (vec)
+      if constexpr (mixed)
+        cg_update_bf16_kernel<<<g, 256, 0, s>>>(n, k.dinv, k.x, k.r, k.p, k.s, k.w, p.cg_st.get(), p.part.get(), vec);
+      else if (vec)
         cg_update_kernel<T, true><<<g, 256, 0, s>>>(n, k.dinv, k.x, k.r, k.p, k.s, k.w, p.cg_st.get(), p.part.get());
       else
         cg_update_kernel<T, false><<<g, 256, 0, s>>>(n, k.dinv, k.x, k.r, k.p, k.s, k.w, p.cg_st.get(),
                                                      p.part.get());
       FEM_LAUNCH_CHECK();
-      cg_apply<T>(p, k, s);
+      cg_apply(p, k, s);
     }
     const CgScalars& st = read_scalars(p, s);
     if (st.done) break;
@@ -574,43 +712,56 @@ double outer_residual(MassPlan& p, const double* f, const double* u, cudaStream_
   return std::sqrt(read_scalars(p, s).res);
 }
 
-// The FP32 inner solve's relative tolerance: what the last cycle still needs
-// (with a factor 2 margin), but not below what FP32 Krylov vectors attain.
-constexpr double kInnerFloor = 5e-6;
+// The inner solves' relative tolerance: what the last cycle still needs (with
+// a factor 2 margin), but not below what the Krylov vectors' storage attains:
+// FP32 (unit roundoff 6e-8) reaches 5e-6; BF16 (unit roundoff 3.9e-3) stalls
+// near its rounding level, so each BF16 cycle asks for 2 decimal digits.
+constexpr double kInnerFloor = 5e-6, kInnerFloorBf16 = 1e-2;
+
+// FP64 outer loop: r = f - M u in FP64, correction d from the inner PCG on
+// r / ||r|| (storage S), u += ||r|| d.
+template <class T, class S>
+void refine(MassPlan& p, const Krylov<T, S>& k, const double* f, double* u, double rtol, int max_iter, double floor,
+            int& total_it, int& outer, double& nf, double& nr, cudaStream_t s) {
+  nf = outer_residual(p, f, nullptr, s);
+  FEM_CUDA_CHECK(cudaMemsetAsync(u, 0, size_t(p.l_size) * sizeof(double), s));
+  nr = nf;
+  while (nr > rtol * nf && total_it < max_iter && outer < 100) {
+    const double inner = std::min(0.5, std::max(floor, 0.5 * rtol * nf / nr));
+    const CgScalars st = krylov_solve<T, S>(p, k, p.cg_r.get(), 1.0 / nr, inner, max_iter - total_it, s);
+    total_it += st.iters;
+    ++outer;
+    add_scaled_kernel<<<red_grid(p.l_size), 256, 0, s>>>(p.l_size, nr, k.x, u);
+    FEM_LAUNCH_CHECK();
+    const double prev = nr;
+    nr = outer_residual(p, f, u, s);
+    if (!(nr < prev)) break;  // no progress: the inner solve has stalled
+  }
+}
 
 SolveStats mass_solve_impl(MassPlan& p, const double* f, double* u, double rtol, int max_iter, int precision,
                            cudaStream_t s) {
-  const bool fp32 = precision == FEM_B200_SOLVE_FP32_IR;
-  ensure_solver_state(p, fp32, s);
+  ensure_solver_state(p, precision, s);
   const SolveDispatch& d = solve_dispatch();
   const int di = p.Q - p.P;
   int total_it = 0, outer = 0;
   double nf = 0.0, nr = 0.0;
-  if (!fp32) {
+  if (precision == FEM_B200_SOLVE_FP64) {
     const Krylov<double> k{u, p.cg_r.get(), p.cg_p.get(), p.cg_s.get(), p.cg_w.get(), p.evec.get(),
                            p.dinv.get(), p.qd_t.get(), d.cg64[p.P][di]};
     const CgScalars st = krylov_solve<double>(p, k, f, 1.0, rtol, max_iter, s);
     total_it = st.iters;
     nf = std::sqrt(st.rr0);
     nr = outer_residual(p, f, u, s);  // the true FP64 residual
-  } else {
-    // FP64 outer loop: r = f - M u in FP64, correction from FP32 PCG on r / ||r||.
-    nf = outer_residual(p, f, nullptr, s);
-    FEM_CUDA_CHECK(cudaMemsetAsync(u, 0, size_t(p.l_size) * sizeof(double), s));
-    nr = nf;
+  } else if (precision == FEM_B200_SOLVE_FP32_IR) {
     const Krylov<float> k{p.f_x.get(), p.f_r.get(), p.f_p.get(), p.f_s.get(), p.f_w.get(), p.evec32.get(),
                           p.dinv32.get(), p.qd_t32.get(), d.cg32[p.P][di]};
-    while (nr > rtol * nf && total_it < max_iter && outer < 50) {
-      const double inner = std::min(0.5, std::max(kInnerFloor, 0.5 * rtol * nf / nr));
-      const CgScalars st = krylov_solve<float>(p, k, p.cg_r.get(), 1.0 / nr, inner, max_iter - total_it, s);
-      total_it += st.iters;
-      ++outer;
-      add_scaled_kernel<<<red_grid(p.l_size), 256, 0, s>>>(p.l_size, nr, p.f_x.get(), u);
-      FEM_LAUNCH_CHECK();
-      const double prev = nr;
-      nr = outer_residual(p, f, u, s);
-      if (!(nr < prev)) break;  // no progress: the FP32 solve has stalled
-    }
+    refine(p, k, f, u, rtol, max_iter, kInnerFloor, total_it, outer, nf, nr, s);
+  } else {
+    const Krylov<float, __nv_bfloat16> k{p.f_x.get(),  p.h_r.get(),    p.h_p.get(),    p.h_s.get(),
+                                         p.f_w.get(),  p.evec32.get(), p.dinv32.get(), p.qd_t16.get(),
+                                         d.cg16[p.P][di]};
+    refine(p, k, f, u, rtol, max_iter, kInnerFloorBf16, total_it, outer, nf, nr, s);
   }
   check_status(p, s);
   SolveStats out;
@@ -645,7 +796,8 @@ int fem_b200_mass_solve(fem_b200_mass op, const double* f, int64_t n_f, double* 
     require(n_f == p.l_size && f && n_u == p.l_size && u, "mass solve: f and u must have l_size entries");
     require(rtol > 0.0 && rtol < 1.0, "mass solve: rtol must be in (0, 1)");
     require(max_iter >= 1, "mass solve: max_iter must be positive");
-    require(precision == FEM_B200_SOLVE_FP64 || precision == FEM_B200_SOLVE_FP32_IR,
+    require(precision == FEM_B200_SOLVE_FP64 || precision == FEM_B200_SOLVE_FP32_IR ||
+                precision == FEM_B200_SOLVE_BF16_IR,
             "mass solve: unknown precision");
     if (p.comp_run != p.num_comp)
       throw unsupported_error(

@@ -337,8 +337,13 @@ int fem_b200_mass_diagonal(fem_b200_mass op, double *diag, int64_t n, void *stre
  *                           correction from FP32 PCG (FP32 qdata, vectors and
  *                           fused apply; FP64 reductions) on r / ||r||, each
  *                           inner solve to what the target still needs (not
- *                           below 5e-6), until ||f - M u|| <= rtol ||f||.
- * max_iter bounds the CG iterations (all inner ones for FP32_IR).  Outputs (any
+ *                           below 5e-6), until ||f - M u|| <= rtol ||f||;
+ *   FEM_B200_SOLVE_BF16_IR  the same refinement with a BF16-storage inner PCG:
+ *                           BF16 qdata and Krylov vectors r, p, s, FP32
+ *                           x, dinv, M z and arithmetic, FP64 reductions; each
+ *                           inner solve to at most 1e-2 (BF16's attainable
+ *                           level), so more refinement steps.
+ * max_iter bounds the CG iterations (all inner ones for the _IR forms).  Outputs (any
  * may be NULL): total CG iterations, refinement steps, and the true FP64
  * relative residual ||f - M u|| / ||f||.  Plans with the deterministic scatter
  * reproduce every bit of u from run to run.  Synchronises the stream.  Plans of the reference apply_mass with num_comp > 1 are
@@ -346,6 +351,7 @@ int fem_b200_mass_diagonal(fem_b200_mass op, double *diag, int64_t n, void *stre
  * No reference counterpart (the reference has no solver). */
 #define FEM_B200_SOLVE_FP64 0
 #define FEM_B200_SOLVE_FP32_IR 1
+#define FEM_B200_SOLVE_BF16_IR 2
 int fem_b200_mass_solve(fem_b200_mass op, const double *f, int64_t n_f, double *u, int64_t n_u, double rtol,
                         int max_iter, int precision, int *iterations, int *refinements, double *rel_residual,
                         void *stream);
