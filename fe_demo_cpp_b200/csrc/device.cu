@@ -153,9 +153,32 @@ void launch_apply3_narrow(const MassPlan& p, const double* u, double* v, double*
   FEM_LAUNCH_CHECK();
 }
 
-// One element per thread (P <= 3): 128-thread CTAs over the plan's elements.
+// Staged element kernel: one-warp CTAs (4 tiles).  ~64M-DoF boxes, one and
+// three components, interleaved runs on one box each: P = 3 unstaged 1.32 /
+// 0.94 ms, staged in 64-thread CTAs 1.24 / 0.77 ms; on another box staged
+// in 32 / 64 / 128-thread CTAs 1.27 / 1.30 / 1.45 ms (one component), 0.755 /
+// 0.77 / 0.91 ms (three), and P = 2 unstaged 2.99 / 1.48 ms, staged in
+// 32-thread CTAs 2.62 / 1.42 ms.
+constexpr int kElemStageCT = 32;
+
+// One element per thread (P <= 3): the staged kernel (qdata and offsets
+// bulk-copied into shared memory per CTA); for unaligned pointers
+// 128-thread CTAs reading them from global memory.
 template <int P, int Q>
 void launch_apply3_element(const MassPlan& p, const double* u, double* v, double* ev, cudaStream_t s) {
+  using LS = ElemStage<P, Q, kElemStageCT>;
+  if (LS::SMEM <= kMaxSmemPerCta && (reinterpret_cast<uintptr_t>(p.offs()) & 15) == 0 &&
+      (reinterpret_cast<uintptr_t>(p.qd()) & 15) == 0) {
+    const auto kern = mass3d_apply_element_staged_kernel<P, Q, kElemStageCT>;
+    static std::atomic<uint64_t> smem_set{0};
+    set_smem(kern, LS::SMEM, smem_set);
+    const int64_t wave = resident_ctas(reinterpret_cast<const void*>(kern), kElemStageCT, LS::SMEM);
+    kern<<<unsigned((p.tiles() + LS::TILES - 1) / LS::TILES), kElemStageCT, LS::SMEM, s>>>(
+        make_mat<P, Q>(p.basis), p.offs(), p.qd(), u, v, ev, p.elems(), p.comp_run, p.comp_stride, wave,
+        p.status.get());
+    FEM_LAUNCH_CHECK();
+    return;
+  }
   const unsigned grid = unsigned((p.tiles() * 8 + 127) / 128);
   const auto kern = mass3d_apply_element_kernel<P, Q>;
   // L2 prefetch a wave ahead at P = 3 (1.05-1.07x); at P = 2 it measured
@@ -253,7 +276,7 @@ struct Table {
     if constexpr (Prefetch3D<P, Q>::SMEM <= kMaxSmemPerCta) pf[P][DQ] = launch_apply3_pf<P, Q>;
     if constexpr (Mass3D<P, Q>::MINB_OCC > 1) oc[P][DQ] = launch_apply3_kernel<P, Q, Mass3D<P, Q>::MINB_OCC, false, false>;
     if constexpr (Narrow3D<P, Q>::SMEM <= kMaxSmemPerCta) nw[P][DQ] = launch_apply3_narrow<P, Q>;
-    if constexpr (P <= 3) el[P][DQ] = launch_apply3_element<P, Q>;  // registers: 86 (P=2), 250 (P=3)
+    if constexpr (P <= 3) el[P][DQ] = launch_apply3_element<P, Q>;  // staged: 67-92 registers (P=2), 156-164 (P=3)
     bd[0][P][DQ] = launch_build1<P, Q>;
     bd[1][P][DQ] = launch_build2<P, Q>;
     bd[2][P][DQ] = launch_build3<P, Q>;
