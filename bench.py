@@ -128,7 +128,24 @@ class RefSample:
         self.plan = self.oracle.RefPlan(self.ref, 3, ne, P, Q, n_loc, local, None, self.threads, coords=coords)
         self.u = np.random.default_rng([SEED, 1]).uniform(-1, 1, n_loc)
         self.v = np.zeros(n_loc)
+        self.local, self.n_loc, self.coords = local, n_loc, coords
         return ne
+
+    def device_parity(self, fem, dev):
+        """Parity guard at the workload's own mesh: the sample's submesh
+        through the device path (fused build, then the fused apply) against
+        the reference's build + operator_apply output of the last timed
+        apply; returns max |v_dev - v_ref| / max |v_ref|."""
+        import torch
+        rx = fem.Restriction(self.ne, P**3, 3, self.n_loc, 3 * self.n_loc, self.local)
+        qd = torch.empty(Q**3 * self.ne, dtype=torch.float64, device=dev)
+        fem.mass_build(rx, fem.Basis(3, 3, P, Q), torch.from_numpy(self.coords).to(dev), qd)
+        op = fem.MassOperator(fem.Restriction(self.ne, P**3, 1, self.n_loc, self.n_loc, self.local),
+                              fem.Basis(3, 1, P, Q), qd, fem.QF.apply_mass)
+        v = torch.empty(self.n_loc, dtype=torch.float64, device=dev)
+        op.apply(torch.from_numpy(self.u).to(dev), v)
+        got = v.cpu().numpy()
+        return float(np.abs(got - self.v).max() / np.abs(self.v).max())
 
     def _time_once(self):
         t0 = time.perf_counter()
@@ -315,6 +332,12 @@ def run_b200(args, rank, world, local_rank):
         "clocks": clocks,
         "gpu_launches": 2 * K * launches,
     }
+    # full-size property after the timed region: 1^T M 1 = the volume of the unit box
+    u.fill_(1.0)
+    op.apply(u, v)
+    vol = float(v.sum())
+    line["parity"] = {"full_size_1tM1": vol, "full_size_1tM1_err": abs(vol - 1.0)}
+    assert abs(vol - 1.0) <= 1e-11, f"1^T M 1 = {vol!r}, not the unit box's volume"
     if rank == 0 and world == 1 and not args.no_orders:
         # after the timed region and the e2e run; the workload's buffers are released first
         del u, v, w, op, ru, bu
@@ -332,6 +355,12 @@ def run_b200(args, rank, world, local_rank):
         line["cpu_baseline"] = {"value": s.gdofs(statistics.median(ts)), "unit": UNIT, "cores": s.threads,
                                 "kind": "reference", "sample": s.describe() + ", median of 3 after 1 warm-up",
                                 "single_core": single_core_baseline(mesh)}
+        # parity guard on the same sample of the workload mesh (outside every timed region)
+        err = s.device_parity(fem, dev)
+        line["parity"].update({"sample": f"first {s.n_slabs} z-slabs of the workload mesh ({s.ne} elements)",
+                               "against": "reference build + operator_apply (oracle/_ref), element-chunked",
+                               "max_rel_err": err, "tol": 1e-12})
+        assert err <= 1e-12, f"device apply differs from the reference on the workload sample: {err:.3e}"
     return line
 
 
