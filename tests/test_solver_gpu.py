@@ -233,3 +233,59 @@ def test_deterministic_solve_is_bitwise_reproducible(fem, cuda, precision):
     for u_h, info in out[1:]:
         assert np.array_equal(u_h, out[0][0])
         assert info == out[0][1]
+
+
+def _oracle_apply_chunked(orc, m, qd_h, u_h, P, Q, slabs=8):
+    """The scalar mass apply of the whole mesh through the oracle, in chunks
+    of z-slabs (each a self-contained mesh, nodes renumbered compactly) run in
+    parallel threads and added into the global vector in chunk order."""
+    import concurrent.futures as cf
+    import os
+    nx, ny, nz = m.shape
+    ne_slab, es, nq = nx * ny, P**3, Q**3
+    bounds = [(z0 * ne_slab, min(nz, z0 + slabs) * ne_slab) for z0 in range(0, nz, slabs)]
+    qd2 = qd_h.reshape(nq, m.num_elem)
+
+    def chunk(lo_hi):
+        lo, hi = lo_hi
+        nodes, local = np.unique(m.offsets[lo * es: hi * es], return_inverse=True)
+        q = np.ascontiguousarray(qd2[:, lo:hi]).reshape(-1)
+        n = int(nodes.size)
+        return nodes, orc.mass_apply(3, hi - lo, P, Q, 1, n, n, local.astype(np.int32), q, u_h[nodes])
+
+    out = np.zeros(m.num_nodes)
+    with cf.ThreadPoolExecutor(max_workers=min(len(bounds), os.cpu_count() or 1)) as ex:
+        for nodes, vloc in ex.map(chunk, bounds):
+            out[nodes] += vloc
+    return out
+
+
+@pytest.mark.parametrize("precision", ["fp32_ir", "bf16_ir", "fp64"])
+def test_full_size_solve_residual_against_oracle(fem, cuda, orc, precision):
+    """The solve benchmark's configuration at its full size: 64^3 hexes, P=5,
+    Q=6, three components (vector mass, 50.9M DoFs), rtol 1e-10.  The true
+    residual ||f - M u|| / ||f|| of the returned u is recomputed with the
+    oracle's apply, component by component over the whole mesh, and must meet
+    rtol (1.05x margin for the two applies' rounding) and agree with the
+    residual the solve reports."""
+    import torch
+    P, Q, nc = 5, 6, 3
+    m = box_mesh((64, 64, 64), P, seed=1)
+    N = m.num_nodes
+    qd = qdata(fem, cuda, m, Q)
+    op = fem.MassOperator(fem.Restriction(m.num_elem, P**3, nc, N, nc * N, m.offsets), fem.Basis(3, nc, P, Q), qd,
+                          fem.QF.apply_mass_vector)
+    g = torch.Generator(device=cuda).manual_seed(1)
+    f = torch.rand(nc * N, dtype=torch.float64, device=cuda, generator=g) * 2 - 1
+    u = torch.empty_like(f)
+    info = op.solve(f, u, rtol=1e-10, max_iter=2000, precision=precision)
+    assert info["rel_residual"] <= 1e-10, info
+    qd_h, u_h, f_h = host(qd), host(u), host(f)
+    del qd, u, f, op
+    res2 = 0.0
+    for k in range(nc):
+        mu = _oracle_apply_chunked(orc, m, qd_h, u_h[k * N:(k + 1) * N], P, Q)
+        res2 += float(np.sum((f_h[k * N:(k + 1) * N] - mu) ** 2))
+    rel = np.sqrt(res2) / np.linalg.norm(f_h)
+    assert rel <= 1.05e-10, (precision, rel, info)
+    assert abs(rel - info["rel_residual"]) <= 0.05 * rel + 1e-14, (rel, info)
