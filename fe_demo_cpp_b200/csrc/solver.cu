@@ -462,7 +462,23 @@ unsigned resident_grid(K kernel, int threads, int smem, int64_t n_tiles) {
 
 // w (+)= M (dinv . r) with delta = (dinv . r)^T M (dinv . r) reduced into the
 // solver scalars.  ev != nullptr: element contributions to the E-vector.
-template <int P, int Q, class T, int NCB, class S = T, bool EO = (P == 4 || P >= 6) && sizeof(T) == 8 && NCB == 1>
+// Where the Krylov apply takes the even-odd contractions (centro-symmetric B).
+// 64^3 hexes, 3 components, one box, direct -> even-odd ms a solve:
+//   FP32 storage  P = 4 17.4 -> 16.8, P = 5 32.0 -> 31.1, P = 6 58.0 -> 58.7,
+//                 P = 7 92.1 -> 89.9;
+//   BF16 storage  P = 4 27.6 -> 19.5, P = 5 41.4 -> 31.3, P = 6 75.4 -> 57.4,
+//                 P = 7 124.0 -> 91.6 (the direct-form BF16 apply stalled 4x
+//                 longer on its loads: 12 against 2.8 long-scoreboard stalls
+//                 per issue at P = 5).
+// FP64 (one component at a time) as the one-tile apply: P = 4 and P >= 6.
+template <int P, class T, class S, int NCB>
+constexpr bool cg_even_odd() {
+  if constexpr (sizeof(T) == 8) return (P == 4 || P >= 6) && NCB == 1;
+  if constexpr (std::is_same<S, __nv_bfloat16>::value) return P >= 4;
+  return P >= 4 && P != 6;
+}
+
+template <int P, int Q, class T, int NCB, class S = T, bool EO = cg_even_odd<P, T, S, NCB>()>
 void launch_cg_apply3(const MassPlan& p, const S* r, T* w, T* ev, const S* qd, const ApplyCg<T>& ext,
                       cudaStream_t s) {
   using L = Mass3D<P, Q>;
@@ -470,7 +486,7 @@ void launch_cg_apply3(const MassPlan& p, const S* r, T* w, T* ev, const S* qd, c
   static std::atomic<uint64_t> smem_set{0};
   // FP64, one component at a time: the even-odd contractions at P = 4 and
   // P >= 6 for a centro-symmetric B (as the one-tile apply), else at P >= 7
-  // the direct form from a shared copy of the matrix.  Last argument: each CTA
+  // the direct form from a shared copy of the matrix (cg_even_odd).  Last argument: each CTA
   // prefetches its next tile into L2 (FP64 solve 57.2 -> 56.5 ms at 64^3,
   // P = 5, 3 components; FP32 unchanged).
   if constexpr (EO) {
