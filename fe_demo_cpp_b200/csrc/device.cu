@@ -102,15 +102,20 @@ int persistent_grid(K kernel, int threads, int smem, int64_t n_tiles) {
   return int(std::min<int64_t>(n_tiles, resident_ctas(reinterpret_cast<const void*>(kernel), threads, smem)));
 }
 
-template <int P, int Q>
+// The pipelined variant, with the even-odd contractions where the one-tile
+// kernel takes them (plain_even_odd, centro-symmetric B).
+template <int P, int Q, bool EO = plain_even_odd<P>()>
 void launch_apply3_pipe(const MassPlan& p, const double* u, double* v, double* ev, cudaStream_t s) {
+  if constexpr (EO) {
+    if (!p.centro_symmetric) return launch_apply3_pipe<P, Q, false>(p, u, v, ev, s);
+  }
   using L = Pipe3D<P, Q>;
+  const auto kern = mass3d_apply_pipe_kernel<P, Q, EO>;
   static std::atomic<uint64_t> smem_set{0};
-  set_smem(mass3d_apply_pipe_kernel<P, Q>, L::SMEM, smem_set);
-  const int grid = persistent_grid(mass3d_apply_pipe_kernel<P, Q>, L::NT, L::SMEM, p.tiles());
-  mass3d_apply_pipe_kernel<P, Q><<<grid, L::NT, L::SMEM, s>>>(make_mat<P, Q>(p.basis), p.offs(),
-                                                               p.qd(), u, v, ev, p.elems(), p.comp_run,
-                                                               p.comp_stride, p.tiles(), p.status.get());
+  set_smem(kern, L::SMEM, smem_set);
+  const int grid = persistent_grid(kern, L::NT, L::SMEM, p.tiles());
+  kern<<<grid, L::NT, L::SMEM, s>>>(make_mat<P, Q>(p.basis), p.offs(), p.qd(), u, v, ev, p.elems(), p.comp_run,
+                                    p.comp_stride, p.tiles(), p.status.get());
   FEM_LAUNCH_CHECK();
 }
 
@@ -343,12 +348,16 @@ ApplyLauncher variant_launcher(const MassPlan& p, int variant) {
 // The variant a plan runs until it is autotuned: where one variant beat the
 // one-tile kernel on every B200 of the order sweep (64M-DoF box meshes,
 // Q = P + 1, one and three components), that one; else the one-tile kernel.
-// element at P <= 3 (P = 2: 2.5x, P = 3: 1.1-1.15x).  Elsewhere the one-tile
-// kernel (with the even-odd contractions at P = 4 and P >= 6 it leads at
-// every order from 4 to 8; the ranking of the others moves from box to box,
-// which the autotuner settles).
+// element at P <= 3 (P = 2: 2.5x, P = 3: 1.1-1.15x).  At P = 6 with a
+// centro-symmetric B the pipelined kernel with the even-odd contractions
+// (0.723 / 0.634 ms against the one-tile kernel's 0.778 / 0.675 ms, one /
+// three components, two interleaved runs on one box; at P = 4 and 7 it
+// trails: 1.054 vs 0.954, 0.752 vs 0.602 ms).  Elsewhere the one-tile kernel
+// (with the even-odd contractions at P = 4 and P >= 6); the ranking of the
+// others moves from box to box, which the autotuner settles.
 int default_variant(const MassPlan& p) {
   if (p.dim == 3 && p.Q == p.P + 1 && p.P <= 3) return FEM_B200_KERNEL_ELEMENT;
+  if (p.dim == 3 && p.P == 6 && p.Q == 7 && p.centro_symmetric) return FEM_B200_KERNEL_PIPELINED;
   return FEM_B200_KERNEL_SIMPLE;
 }
 

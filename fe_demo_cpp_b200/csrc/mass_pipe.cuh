@@ -90,7 +90,9 @@ struct Pipe3D {
   static constexpr int SMEM = QD_BYTES + AB_BYTES + OFF_BYTES + 8 * (NOFF + NQD);
 };
 
-template <int P, int Q>
+// EO: the even-odd contractions (eo_fwd / eo_bwd, centro-symmetric B) in
+// place of the direct sums, in all six passes.
+template <int P, int Q, bool EO = false>
 __global__ void __launch_bounds__(Pipe3D<P, Q>::NT) mass3d_apply_pipe_kernel(
     const __grid_constant__ Mat1D<P, Q> m, const int* __restrict__ offs, const double* __restrict__ qd,
     const double* __restrict__ u, double* __restrict__ v, double* __restrict__ ev, int num_elem, int num_comp_run,
@@ -176,13 +178,20 @@ __global__ void __launch_bounds__(Pipe3D<P, Q>::NT) mass3d_apply_pipe_kernel(
       const int64_t ks = k * comp_stride;
       if (nodal) {  // phase A: z
         const int px = col % P, py = col / P;
+        double o[Q];
+        if constexpr (EO) {
+          eo_fwd<P, Q>(m, x, o);
+        } else {
 #pragma unroll
-        for (int qz = 0; qz < Q; ++qz) {
-          double s = 0.0;
+          for (int qz = 0; qz < Q; ++qz) {
+            double s = 0.0;
 #pragma unroll
-          for (int pz = 0; pz < P; ++pz) s += m.B[qz * P + pz] * x[pz];
-          sa[py * M::PS1 + (qz * P + px) * E + e] = s;
+            for (int pz = 0; pz < P; ++pz) s += m.B[qz * P + pz] * x[pz];
+            o[qz] = s;
+          }
         }
+#pragma unroll
+        for (int qz = 0; qz < Q; ++qz) sa[py * M::PS1 + (qz * P + px) * E + e] = o[qz];
       }
       __syncthreads();
       if (mixed) {  // phase B: y
@@ -190,13 +199,20 @@ __global__ void __launch_bounds__(Pipe3D<P, Q>::NT) mass3d_apply_pipe_kernel(
 #pragma unroll
         for (int py = 0; py < P; ++py) y[py] = sa[py * M::PS1 + col * E + e];
         const int px = col % P, qz = col / P;
+        double o[Q];
+        if constexpr (EO) {
+          eo_fwd<P, Q>(m, y, o);
+        } else {
 #pragma unroll
-        for (int qy = 0; qy < Q; ++qy) {
-          double s = 0.0;
+          for (int qy = 0; qy < Q; ++qy) {
+            double s = 0.0;
 #pragma unroll
-          for (int py = 0; py < P; ++py) s += m.B[qy * P + py] * y[py];
-          sb[px * M::PS2 + (qz * Q + qy) * E + e] = s;
+            for (int py = 0; py < P; ++py) s += m.B[qy * P + py] * y[py];
+            o[qy] = s;
+          }
         }
+#pragma unroll
+        for (int qy = 0; qy < Q; ++qy) sb[px * M::PS2 + (qz * Q + qy) * E + e] = o[qy];
       }
       if (k == 0) {  // this tile's qdata and the next tile's offsets (issued an iteration ago)
         bool ok = wait_qd(it);
@@ -228,20 +244,30 @@ __global__ void __launch_bounds__(Pipe3D<P, Q>::NT) mass3d_apply_pipe_kernel(
 #pragma unroll
         for (int px = 0; px < P; ++px) w[px] = sb[px * M::PS2 + col * E + e];
         double r[Q];
-#pragma unroll
-        for (int qx = 0; qx < Q; ++qx) {
-          double s = 0.0;
-#pragma unroll
-          for (int px = 0; px < P; ++px) s += m.B[qx * P + px] * w[px];
-          r[qx] = qs[(qx * Q * Q + col) * E + e] * s;
-        }
         const int qy = col % Q, qz = col / Q;
+        if constexpr (EO) {
+          double t[Q], o[P];
+          eo_fwd<P, Q>(m, w, t);
 #pragma unroll
-        for (int px = 0; px < P; ++px) {
-          double s = 0.0;
+          for (int qx = 0; qx < Q; ++qx) r[qx] = qs[(qx * Q * Q + col) * E + e] * t[qx];
+          eo_bwd<P, Q>(m, r, o);
 #pragma unroll
-          for (int qx = 0; qx < Q; ++qx) s += m.B[qx * P + px] * r[qx];
-          sa[qy * M::PS3 + (qz * P + px) * E + e] = s;
+          for (int px = 0; px < P; ++px) sa[qy * M::PS3 + (qz * P + px) * E + e] = o[px];
+        } else {
+#pragma unroll
+          for (int qx = 0; qx < Q; ++qx) {
+            double s = 0.0;
+#pragma unroll
+            for (int px = 0; px < P; ++px) s += m.B[qx * P + px] * w[px];
+            r[qx] = qs[(qx * Q * Q + col) * E + e] * s;
+          }
+#pragma unroll
+          for (int px = 0; px < P; ++px) {
+            double s = 0.0;
+#pragma unroll
+            for (int qx = 0; qx < Q; ++qx) s += m.B[qx * P + px] * r[qx];
+            sa[qy * M::PS3 + (qz * P + px) * E + e] = s;
+          }
         }
       }
       __syncthreads();
@@ -250,24 +276,41 @@ __global__ void __launch_bounds__(Pipe3D<P, Q>::NT) mass3d_apply_pipe_kernel(
 #pragma unroll
         for (int qy = 0; qy < Q; ++qy) y[qy] = sa[qy * M::PS3 + col * E + e];
         const int px = col % P, qz = col / P;
+        double o[P];
+        if constexpr (EO) {
+          eo_bwd<P, Q>(m, y, o);
+        } else {
 #pragma unroll
-        for (int py = 0; py < P; ++py) {
-          double s = 0.0;
+          for (int py = 0; py < P; ++py) {
+            double s = 0.0;
 #pragma unroll
-          for (int qy = 0; qy < Q; ++qy) s += m.B[qy * P + py] * y[qy];
-          sb[qz * M::PS4 + (py * P + px) * E + e] = s;
+            for (int qy = 0; qy < Q; ++qy) s += m.B[qy * P + py] * y[qy];
+            o[py] = s;
+          }
         }
+#pragma unroll
+        for (int py = 0; py < P; ++py) sb[qz * M::PS4 + (py * P + px) * E + e] = o[py];
       }
       __syncthreads();
       if (nodal) {  // phase G: z^T and the scatter
         double z[Q];
 #pragma unroll
         for (int qz = 0; qz < Q; ++qz) z[qz] = sb[qz * M::PS4 + col * E + e];
+        double o[P];
+        if constexpr (EO) {
+          eo_bwd<P, Q>(m, z, o);
+        } else {
+#pragma unroll
+          for (int pz = 0; pz < P; ++pz) {
+            double s = 0.0;
+#pragma unroll
+            for (int qz = 0; qz < Q; ++qz) s += m.B[qz * P + pz] * z[qz];
+            o[pz] = s;
+          }
+        }
 #pragma unroll
         for (int pz = 0; pz < P; ++pz) {
-          double s = 0.0;
-#pragma unroll
-          for (int qz = 0; qz < Q; ++qz) s += m.B[qz * P + pz] * z[qz];
+          const double s = o[pz];
           if (valid) {
             if (ev)
               ev[(int64_t(k) * M::ES + pz * P * P + col) * num_elem + eg] = s;
