@@ -325,7 +325,7 @@ constexpr int batch_min_blocks(int P, int threads, int ncb, bool shared_matrix =
 
 // FP64 classes at P = 4 and P >= 6, FP32 classes from P = 6 (512 uneven meshes,
 // FP32: 113.0 -> 116.4 GDoF/s), use the even-odd contractions when their
-// B is centro-symmetric (as the single-mesh one-tile kernel, plain_even_odd;
+// B is centro-symmetric (as the single-mesh one-tile kernel at those orders;
 // P = 7 with two resident CTAs); otherwise the direct form, from a shared
 // copy of the matrix at P >= 7.
 template <int P, int Q, class T, int NCB, bool EO = (sizeof(T) == 8 ? (P == 4 || P >= 6) : P >= 6) && NCB == 1>

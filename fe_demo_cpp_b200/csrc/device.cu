@@ -63,11 +63,13 @@ constexpr bool plain_shared_matrix() {
 // a centro-symmetric B: P = 4 1.10x, P = 6 1.53x (68 registers without spills
 // instead of 72 with 84 B), P = 7 1.85x and P = 8 1.47x against the
 // shared-matrix form (the folds are half of B, so holding them in registers
-// no longer starves the CTA: P = 7 two CTAs at 64 registers, no spills); P = 5
-// equal, so it keeps the direct form.
+// no longer starves the CTA: P = 7 two CTAs at 64 registers, no spills).
+// P = 5: equal in short bursts at full clock, but 1.026x over the bench's
+// sustained 200-launch region, where the power cap sets the clock (fewer
+// FP64 operations: 0.847 -> 0.825 ms at 1680-1810 MHz, two interleaved runs).
 template <int P>
 constexpr bool plain_even_odd() {
-  return P == 4 || P >= 6;
+  return P >= 4;
 }
 
 template <int P, int Q, int MINB, bool SB, bool EO>
