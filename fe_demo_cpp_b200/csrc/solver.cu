@@ -470,10 +470,11 @@ unsigned resident_grid(K kernel, int threads, int smem, int64_t n_tiles) {
 //                 P = 7 124.0 -> 91.6 (the direct-form BF16 apply stalled 4x
 //                 longer on its loads: 12 against 2.8 long-scoreboard stalls
 //                 per issue at P = 5).
-// FP64 (one component at a time) as the one-tile apply: P = 4 and P >= 6.
+// FP64 (one component at a time) as the one-tile apply: P >= 4 (P = 5 51.6
+// -> 50.7 ms a solve).
 template <int P, class T, class S, int NCB>
 constexpr bool cg_even_odd() {
-  if constexpr (sizeof(T) == 8) return (P == 4 || P >= 6) && NCB == 1;
+  if constexpr (sizeof(T) == 8) return P >= 4 && NCB == 1;
   if constexpr (std::is_same<S, __nv_bfloat16>::value) return P >= 4;
   return P >= 4 && P != 6;
 }
