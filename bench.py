@@ -808,9 +808,11 @@ def run_serve(args):
     lines = []
     for prec in ("fp32_ir", "fp64"):
         with fem.Server(slots=args.serve_slots, hbm_budget=budget) as srv:
-            # warm-up: one request of each order (kernel attributes, pool)
+            # warm-up: one request of each order and component count the stream
+            # draws (kernels loaded on first use, kernel attributes, pool)
             for Pw in range(2, 7):
-                srv.wait(srv.submit_box(3, (8, 8, 8), Pw, num_comp=3, seed=1, precision=prec))
+                for ncw in (1, 3):
+                    srv.wait(srv.submit_box(3, (8, 8, 8), Pw, num_comp=ncw, seed=1, precision=prec))
             for rate in rates:
                 rng = np.random.default_rng([SEED, int(rate)])
                 gaps = rng.exponential(1.0 / rate, len(reqs))
