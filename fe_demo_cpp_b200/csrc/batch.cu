@@ -324,11 +324,14 @@ constexpr int batch_min_blocks(int P, int threads, int ncb, bool shared_matrix =
 }
 
 // FP64 classes from P = 4 (512 uneven meshes: P = 5 added 69.6 -> 70.5
-// GDoF/s), FP32 classes from P = 6 (FP32: 113.0 -> 116.4 GDoF/s), use the
-// even-odd contractions when their B is centro-symmetric (as the single-mesh
-// one-tile kernel at those orders; P = 7 with two resident CTAs); otherwise
-// the direct form, from a shared copy of the matrix at P >= 7.
-template <int P, int Q, class T, int NCB, bool EO = (sizeof(T) == 8 ? P >= 4 : P >= 6) && NCB == 1>
+// GDoF/s), FP32 classes from P = 6 with one component at a time (FP32: 113.0
+// -> 116.4 GDoF/s) and at P = 4, 5 also with components batched (116.4 ->
+// 119.0 GDoF/s), use the even-odd contractions when their B is
+// centro-symmetric (as the single-mesh one-tile kernel at those orders; P = 7
+// with two resident CTAs); otherwise the direct form, from a shared copy of
+// the matrix at P >= 7.
+template <int P, int Q, class T, int NCB,
+          bool EO = sizeof(T) == 8 ? P >= 4 && NCB == 1 : (P == 4 || P == 5 || (P >= 6 && NCB == 1))>
 unsigned launch_batch3(const BatchClass& c, const void* meshes, unsigned grid, cudaStream_t s) {
   if constexpr (EO) {
     if (!c.centro_symmetric) return launch_batch3<P, Q, T, NCB, false>(c, meshes, grid, s);
