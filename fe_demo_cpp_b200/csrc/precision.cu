@@ -51,11 +51,13 @@ using LowpLauncher = void (*)(const MassPlan&, const S*, const S*, float*, float
 
 // The even-odd contractions (centro-symmetric B) where they measured faster in
 // single precision (interleaved A/B against the direct form, ~64M DoFs): 3D
-// P = 7 (FP32 1.21x, BF16 1.15x one component), P = 8 (1.04-1.07x) and BF16
-// at P = 6 (1.10x; FP32 there 0.82x); 2D only P = 8 (1.06-1.28x).
+// P = 5 (FP32 0.576 -> 0.522 ms, BF16 0.604 -> 0.555 one component; three
+// components alike), P = 7 (FP32 1.21x, BF16 1.15x), P = 8 (1.04-1.07x) and
+// BF16 at P = 4 (0.878 -> 0.839 ms; FP32 there 0.711 -> 0.765) and P = 6
+// (1.10x; FP32 there 0.82x); 2D only P = 8 (1.06-1.28x).
 template <int P, class S>
 constexpr bool lowp_even_odd_3d() {
-  return P >= 7 || (P == 6 && std::is_same<S, __nv_bfloat16>::value);
+  return P == 5 || P >= 7 || ((P == 4 || P == 6) && std::is_same<S, __nv_bfloat16>::value);
 }
 
 template <int P, int Q, class S, bool EO = lowp_even_odd_3d<P, S>() || P == 8>
