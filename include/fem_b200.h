@@ -58,14 +58,14 @@ extern "C" {
 #define FEM_B200_QF_APPLY_MASS 0        /* include/qfunctions/mass.hpp:45-51: component 0 only */
 #define FEM_B200_QF_APPLY_MASS_VECTOR 1 /* every component: v_k = qdata * u_k (no reference counterpart) */
 /* Kernel variants of the fused 3D mass apply (fem_b200_mass_set_kernel) */
-#define FEM_B200_KERNEL_AUTO 0      /* the autotuned variant for the shape (fem_b200_mass_autotune), else a measured per-order default (3D, Q = P+1: ELEMENT at P <= 3; SIMPLE otherwise) */
+#define FEM_B200_KERNEL_AUTO 0      /* the autotuned variant for the shape (fem_b200_mass_autotune), else a measured per-order default (3D, Q = P+1: ELEMENT at P <= 3, PIPELINED at P = 6 with a centro-symmetric basis; SIMPLE otherwise) */
 #define FEM_B200_KERNEL_SIMPLE 1    /* one CTA per 8-element tile, one element per thread */
 #define FEM_B200_KERNEL_PIPELINED 2 /* persistent CTAs, next tile staged by bulk copies during this one */
 #define FEM_B200_KERNEL_PAIRED 3    /* one CTA per 16 elements, two adjacent elements per thread */
 #define FEM_B200_KERNEL_PREFETCH 4  /* persistent CTAs, qdata bulk-copied two tiles ahead, offsets/u one ahead */
 #define FEM_B200_KERNEL_OCCUPANCY 5 /* as SIMPLE, registers capped for up to 5 resident CTAs per SM */
 #define FEM_B200_KERNEL_NARROW 6    /* half-tile CTAs of 4 elements: twice the registers a thread (high order) */
-#define FEM_B200_KERNEL_ELEMENT 7   /* one element per thread in registers, no shared memory (P <= 3) */
+#define FEM_B200_KERNEL_ELEMENT 7   /* one element per thread in registers (P <= 3); the CTA's qdata and offsets bulk-copied into shared memory first */
 
 typedef struct fem_b200_restriction_s *fem_b200_restriction;
 typedef struct fem_b200_basis_s *fem_b200_basis;
