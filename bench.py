@@ -921,6 +921,25 @@ def run_restriction(args):
         results[(mode, "reference-cuda")] = timed(lambda: ref.apply(True))
         ref.close()
         del ours, e_out, l_out
+    del l_dev, e_dev
+    # the fused operator apply with each scatter (zero v + kernel [+ the
+    # deterministic E-vector reduction]): the deterministic mode's cost
+    x = torch.from_numpy(mesh.coords).to(dev)
+    qd = torch.empty(Q**3 * ne, dtype=torch.float64, device=dev)
+    fem.mass_build(fem.Restriction(ne, es, 3, N, 3 * N, mesh.offsets), fem.Basis(3, 3, P, Q), x, qd)
+    del x
+    u = torch.from_numpy(l_host).to(dev)
+    v = torch.empty_like(u)
+    apply_ms = {}
+    for det in (0, 1):
+        op = fem.MassOperator(fem.Restriction(ne, es, 1, N, N, mesh.offsets, det), fem.Basis(3, 1, P, Q), qd)
+        apply_ms[det] = timed(lambda: op.apply(u, v))
+        del op
+    print(json.dumps({"apply": "mass", "scatter_atomic_ms": apply_ms[0], "scatter_deterministic_ms": apply_ms[1],
+                      "deterministic_over_atomic": apply_ms[1] / apply_ms[0],
+                      "config": {"mesh": "x".join(map(str, SHAPE)), "P": P, "Q": Q, "num_comp": 1, "dofs": N,
+                                 "note": "public apply: v zeroed + fused kernel (+ E-vector transpose-map "
+                                         "reduction in the deterministic mode)"}}), flush=True)
     for (mode, impl), ms in results.items():
         ab = bytes_gather if mode == "gather" else bytes_scatter
         other = results[(mode, "reference-cuda" if impl == "b200" else "b200")]
