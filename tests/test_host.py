@@ -30,6 +30,17 @@ def test_library_exports_every_declared_symbol(fem):
     assert sorted(_lib.SIGNATURES) == syms
 
 
+def test_python_constants_match_the_header():
+    """The Python mirror's solve precisions and kernel variants carry the
+    header's values (FEM_B200_SOLVE_*, FEM_B200_KERNEL_*)."""
+    from fe_demo_cpp_b200.api import SOLVE_PRECISIONS, KernelVariant
+    text = open(os.path.join(ROOT, "include", "fem_b200.h")).read()
+    solve = {k.lower(): int(v) for k, v in re.findall(r"#define FEM_B200_SOLVE_(\w+) (\d+)", text)}
+    assert solve == SOLVE_PRECISIONS
+    kern = {k.lower(): int(v) for k, v in re.findall(r"#define FEM_B200_KERNEL_(\w+) (\d+)", text)}
+    assert kern == {v.name: int(v) for v in KernelVariant}
+
+
 def test_loads_without_gpu_and_reports_device_count(fem):
     n = fem.load().fem_b200_device_count()
     assert n >= 0
